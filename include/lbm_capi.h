@@ -1,0 +1,239 @@
+/*
+ * lbm_capi.h -- C-ABI of the B200-native D3Q19 lattice-Boltzmann library
+ * (liblbm_b200.so).  Plain pointers and sizes only; every call returns an int
+ * status (LBM_OK == 0) and never throws; lbm_last_error() holds the message of
+ * the last failure on the calling thread.
+ *
+ * Each entry cites the reference interface (yagise/MyFluidSimulation, path
+ * inside that project) that it replaces.  The reference's solver classes
+ * LBM3D_Legacy / LBM3D_Home / LBM3D_Hybrid map onto one opaque lbm_solver
+ * created with a method; include/lbm3d_compat.hpp rebuilds those classes on
+ * top of this ABI for C++ callers.
+ *
+ * Threading and streams: a solver is bound to one CUDA stream (its own, or
+ * the one passed in lbm_options.stream) and is not thread-safe.  lbm_step is
+ * asynchronous on that stream; lbm_synchronize waits for it.  Device pointers
+ * returned by getters are borrowed and stay valid until the next lbm_step,
+ * lbm_reset/lbm_reinit_from_macro or lbm_destroy (the HOME method swaps its
+ * moment buffers on every step, as the reference does).
+ */
+#ifndef LBM_CAPI_H
+#define LBM_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+enum {
+    LBM_OK = 0,
+    LBM_ERR_INVALID = 1,      /* bad argument, size or state */
+    LBM_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    LBM_ERR_ALLOC = 3,        /* device or host allocation failed */
+    LBM_ERR_SIZE = 4,         /* a size overflows the supported range */
+    LBM_ERR_IO = 5,           /* file could not be read or written */
+    LBM_ERR_UNSUPPORTED = 6,  /* combination not implemented */
+    LBM_ERR_TIMEOUT = 7       /* a bounded device-side wait gave up */
+};
+
+/* collision / update method (the reference's three solver classes) */
+enum { LBM_METHOD_LEGACY = 0, LBM_METHOD_HOME = 1, LBM_METHOD_HYBRID = 2 };
+/* storage of populations (Legacy/Hybrid) or moments (HOME) */
+enum { LBM_STORE_F32 = 0, LBM_STORE_F16 = 1, LBM_STORE_BF16 = 2 };
+/* boundary: fully periodic (the reference), or a duct along x with a
+ * velocity inlet at x=0 and a zero-gradient outlet at x=Nx-1 */
+enum { LBM_BC_PERIODIC = 0, LBM_BC_DUCT = 1 };
+/* bounce-back at solid cells.
+ * HALFWAY: link-wise halfway bounce-back, a population leaving along c_q comes
+ *   back along -c_q (every population written once per step; the in-place
+ *   AA kernels).
+ * REFERENCE: the reference's own opposite table (src/lbm/lbm3d_legacy.cu:29-32),
+ *   which pairs each diagonal direction with its mirror image in x or y
+ *   rather than its opposite.  Legacy/Hybrid then keep the reference's two
+ *   buffers: a slot nobody writes keeps the previous buffer's value, and a slot
+ *   written both by streaming and by a reflection (a race in the reference)
+ *   takes the reflection.  HOME uses the table deterministically, as the
+ *   reference does.  F32 storage only for Legacy/Hybrid. */
+enum { LBM_BOUNCE_HALFWAY = 0, LBM_BOUNCE_REFERENCE = 1 };
+/* mask byte: any nonzero value is solid (the reference's convention);
+ * bit 3 marks a solid cell as a wall that the drag sum leaves out */
+enum { LBM_MASK_SOLID = 1, LBM_MASK_WALL = 8 };
+/* lbm_get_stats slots */
+enum {
+    LBM_STAT_MASS = 0,   /* sum of rho over fluid cells */
+    LBM_STAT_KE = 1,     /* sum over all cells of |u|^2/2 (divide by N for the mean) */
+    LBM_STAT_DRAG_X = 2, /* momentum exchanged with obstacle cells in one step */
+    LBM_STAT_DRAG_Y = 3,
+    LBM_STAT_DRAG_Z = 4,
+    LBM_STAT_MOM_X = 5,  /* sum of rho*u over fluid cells */
+    LBM_STAT_MOM_Y = 6,
+    LBM_STAT_MOM_Z = 7,
+    LBM_NSTAT = 8
+};
+
+/* Mirrors struct Domain (src/lbm/lbm_common.hpp:6-10). */
+typedef struct lbm_domain {
+    int32_t nx, ny, nz;
+    float tau;
+    float force_x, force_y, force_z;
+} lbm_domain;
+
+typedef struct lbm_options {
+    int32_t method;    /* LBM_METHOD_* */
+    int32_t storage;   /* LBM_STORE_* */
+    int32_t bc;        /* LBM_BC_* */
+    int32_t bounce;    /* LBM_BOUNCE_* */
+    float inlet_u;     /* duct inlet velocity (x) */
+    float rho0;        /* reference density of the shifted F16/BF16 storage (default 1) */
+    void* stream;      /* cudaStream_t to run on; NULL creates one per solver */
+} lbm_options;
+
+typedef struct lbm_solver lbm_solver;
+
+/* Last error message of the calling thread ("" when none). */
+const char* lbm_last_error(void);
+/* Library version string. */
+const char* lbm_version(void);
+
+/* ---- solver lifecycle -------------------------------------------------- */
+
+/* Allocates and resets a solver (rho=1, u=0 equilibrium, no solid cells;
+ * with LBM_BOUNCE_REFERENCE the second population buffer starts as zeros).
+ * Replaces LBM3D_Legacy::init (src/lbm/lbm3d_legacy.cu:141-147),
+ * LBM3D_Home::init (src/lbm/lbm3d_home.cu:301-307) and
+ * LBM3D_Hybrid::init (src/lbm/lbm3d_hybrid.cu:210-221). opts may be NULL
+ * (Legacy, F32, periodic). */
+int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out);
+/* Replaces the destructors (~LBM3D_*, lbm3d_legacy.cu:14, home.cu:5, hybrid.cu:5). */
+int lbm_destroy(lbm_solver* s);
+
+/* Nx*Ny*Nz bytes, x fastest.  Replaces setSolidMask (lbm3d_legacy.cu:149-151,
+ * lbm3d_home.cu:309-311, lbm3d_hybrid.cu:223-225). */
+int lbm_set_solid_mask(lbm_solver* s, const uint8_t* host_mask);
+/* Hybrid only: per-cell BGK-band flags (NULL clears the band).  Replaces
+ * LBM3D_Hybrid::setLegacyMapping (lbm3d_hybrid.cu:227-235); the reference's
+ * second (slot) argument is ignored there and has no counterpart here. */
+int lbm_set_legacy_mapping(lbm_solver* s, const uint8_t* host_is_legacy);
+/* Hybrid only: builds the band on the GPU from the current mask, exactly as
+ * build_distance_to_solid_6n + build_legacy_mask_from_distance
+ * (src/apps/sim_runner.hpp:28-91) with maxDist=max(1,d0) (sim_runner.hpp:221-224).
+ * n_band (may be NULL) receives the number of band cells. */
+int lbm_build_band(lbm_solver* s, int d0, int64_t* n_band);
+/* Copies the band flags out (Nx*Ny*Nz bytes, 1 = BGK band). */
+int lbm_get_band(lbm_solver* s, uint8_t* host_is_legacy);
+
+/* rho=1, u=0 equilibrium.  Replaces reset() (lbm3d_legacy.cu:153-159,
+ * lbm3d_home.cu:313-319, lbm3d_hybrid.cu:237-243). */
+int lbm_reset(lbm_solver* s);
+/* Equilibrium from DEVICE macro fields; NULL velocity components are 0.
+ * NULL rho: Legacy resets (lbm3d_legacy.cu:174-178), HOME and Hybrid use rho=1
+ * (lbm3d_home.cu:119, lbm3d_hybrid.cu:76).  Replaces reinitEquilibriumFromMacro
+ * (lbm3d_legacy.cu:160-208, lbm3d_home.cu:321-333, lbm3d_hybrid.cu:245-257). */
+int lbm_reinit_from_macro(lbm_solver* s, const float* d_rho, const float* d_ux,
+                          const float* d_uy, const float* d_uz);
+/* Same, from HOST arrays (each Nx*Ny*Nz floats; NULL as above): copies them to
+ * the solver's macro buffers on its stream, then reinitialises. */
+int lbm_reinit_from_host(lbm_solver* s, const float* rho, const float* ux,
+                         const float* uy, const float* uz);
+
+/* Advances `substeps` steps, asynchronously on the solver's stream.  The
+ * macro fields (and, when enabled, the statistics) are those of the last
+ * substep, as in the reference, where they hold the moments of the state the
+ * step started from (Legacy/Hybrid, lbm3d_legacy.cu:78-113) or of the state it
+ * produced (HOME, lbm3d_home.cu:275-285).  Replaces step(int)
+ * (lbm3d_legacy.cu:210-224, lbm3d_home.cu:335-354, lbm3d_hybrid.cu:259-283). */
+int lbm_step(lbm_solver* s, int substeps);
+/* Waits for all work queued on the solver's stream. */
+int lbm_synchronize(lbm_solver* s);
+/* Replaces setForce (lbm3d_legacy.hpp:36, lbm3d_home.hpp:32, lbm3d_hybrid.hpp:38). */
+int lbm_set_force(lbm_solver* s, float fx, float fy, float fz);
+/* Hybrid only: the relaxation rate of the non-band ("HOME form") cells'
+ * shear term.  The reference fixes it to 1/tau (lbm3d_hybrid.cu:264-267),
+ * which is the default here too. */
+int lbm_set_shear_omega(lbm_solver* s, float omega_shear);
+
+/* Borrowed device pointers of the macro fields.  Replaces d_rho/d_u/d_v/d_w
+ * (lbm3d_legacy.cu:229-236, lbm3d_home.cu:355-362, lbm3d_hybrid.hpp:45-52). */
+int lbm_macro_ptrs(lbm_solver* s, float** d_rho, float** d_u, float** d_v, float** d_w);
+/* Copies the macro fields to host arrays (any may be NULL); synchronous. */
+int lbm_get_macros(lbm_solver* s, float* rho, float* ux, float* uy, float* uz);
+/* Copies the state to a host array in the reference's layout: Legacy/Hybrid
+ * the 19*N populations f[q*N+id] (what d_f() points at, lbm3d_legacy.cu:225);
+ * HOME the 10*N moments m[k*N+id] (lbm3d_home.hpp:57-71).  Synchronous. */
+int lbm_get_state(lbm_solver* s, float* host_out);
+/* Nx, Ny, Nz and N (any may be NULL).  Replaces Nx()/Ny()/Nz()/N(). */
+int lbm_dims(lbm_solver* s, int32_t* nx, int32_t* ny, int32_t* nz, int64_t* n);
+/* Steps taken since the last reset/reinit. */
+int lbm_step_count(lbm_solver* s, int64_t* steps);
+
+/* Enables (1) or disables (0) the FP64 statistics of the last substep of
+ * every lbm_step (mass, kinetic energy, momentum, momentum-exchange drag). */
+int lbm_enable_stats(lbm_solver* s, int enable);
+/* Synchronises and copies the LBM_NSTAT statistics of the last step that
+ * computed them.  No reference counterpart (the reference sums on the host,
+ * src/bench/main_taylor_green.cpp:157-182). */
+int lbm_get_stats(lbm_solver* s, double* out);
+
+/* Captures `substeps` steps into a CUDA graph on first use and replays it;
+ * same result as lbm_step.  Invalidated by any setter. */
+int lbm_step_graph(lbm_solver* s, int substeps);
+
+/* ---- geometry (host in, host out) ------------------------------------- */
+
+/* STL loader: ASCII when the file starts with "solid" (falls back to binary
+ * if no vertex parses), binary otherwise.  Replaces load_stl
+ * (src/geom/stl_loader.cpp:102-122).  *tris receives 9 floats per triangle
+ * (free with lbm_free); bb receives {min xyz, max xyz}.  LBM_ERR_IO when the
+ * reference would return false. */
+int lbm_load_stl(const char* path, float** tris, int64_t* ntri, float* bb);
+void lbm_free(void* p);
+
+/* Voxel options, mirroring VoxelParams (src/geom/voxelize.hpp:16-24). */
+typedef struct lbm_voxel_params {
+    int32_t nx, ny, nz;
+    float uniform_scale;   /* default 0.9 in VoxelParams, 0.5 on the CLI */
+    float translate[3];
+    int32_t refine;        /* supersampling factor (AMR), >=1 */
+    float coverage_threshold;
+} lbm_voxel_params;
+
+/* GPU voxelizer: fit to the unit cube, SAT surface marking, exterior flood
+ * fill, optional refine^3 coverage downsample.  Bit-exact with
+ * voxelize_mesh_to_mask (src/geom/voxelize.cpp:228-243).  bb may be NULL
+ * (computed from the vertices the way the loader does).  mask_out: Nx*Ny*Nz
+ * bytes, 1 = solid. */
+int lbm_voxelize(const float* tris, int64_t ntri, const float* bb,
+                 const lbm_voxel_params* p, uint8_t* mask_out);
+
+/* ---- free functions of the reference (same names and signatures) ------ */
+
+/* f_i = feq(rho,u) for N cells into d_f (SoA q*N+i); NULL u components are 0.
+ * src/lbm/lbm_reinit.cu:52-61.  Launches on the default stream. */
+void reinit_equilibrium_from_macro(const float* d_rho, const float* d_ux, const float* d_uy,
+                                   const float* d_uz, float* d_f, int N);
+/* |u| per cell.  src/fields/field_ops.cu:25-28. */
+void launch_speed(const float* u, const float* v, const float* w, float* out, int N);
+/* Initial density profiles (--init gauss|slab).  src/fields/init_profiles.cu:31-45. */
+void make_rho_gauss(float* d_rho, int Nx, int Ny, int Nz, float cx, float cy, float cz,
+                    float sigma, float amp);
+void make_rho_slab(float* d_rho, int Nx, int Ny, int Nz, int axis, float amp, float center,
+                   float width);
+/* ASCII legacy VTK (STRUCTURED_POINTS) from a DEVICE field, byte-identical to
+ * src/moment_vtk_writer.cu:9-49.  Throwing on an unopenable file, as the
+ * reference does, is replaced by an error message on stderr. */
+void write_scalar_vtk(const char* filename, const float* d_field, int Nx, int Ny, int Nz);
+void write_vector_vtk(const char* filename, const float* d_fx, const float* d_fy,
+                      const float* d_fz, int Nx, int Ny, int Nz);
+/* Same writers with a status code (LBM_ERR_IO when the file cannot be opened). */
+int lbm_write_scalar_vtk(const char* filename, const float* d_field, int Nx, int Ny, int Nz);
+int lbm_write_vector_vtk(const char* filename, const float* d_fx, const float* d_fy,
+                         const float* d_fz, int Nx, int Ny, int Nz);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* LBM_CAPI_H */

@@ -1,0 +1,559 @@
+// The solver object behind the C-ABI of include/lbm_capi.h.
+//
+// One lbm_solver replaces the reference's three classes (src/lbm/lbm3d_legacy.hpp,
+// lbm3d_home.hpp, lbm3d_hybrid.hpp).  Memory per cell:
+//   Legacy/Hybrid: one population buffer (AA pattern), 19 x 4 B (F32) or 19 x 2 B
+//                  (F16/BF16), plus rho,u,v,w (16 B), mask, flags (1 B each) and a
+//                  link word (4 B); the reference holds two population buffers.
+//   HOME:          two moment buffers of 10 x 4 B (or 10 x 2 B), as the reference.
+// All launches go to the solver's stream; nothing synchronises except the
+// calls documented as synchronous.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_capi.h"
+#include "lbm_internal.h"
+
+namespace lbm {
+
+thread_local std::string g_error;
+void set_error(const std::string& msg) { g_error = msg; }
+
+}  // namespace lbm
+
+using lbm::set_error;
+
+struct lbm_solver {
+    lbm_domain dom{};
+    int method = 0, storage = 0, bc = 0, bounce = 0;
+    float u_in = 0.f, rho0 = 1.f;
+    float omega = 0.f, omega_s = 0.f;
+    int64_t N = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t esize = 4;
+
+    void* f = nullptr;          // AA populations (reference bounce: buffer A)
+    void* f2 = nullptr;         // reference bounce only: buffer B
+    void* m[2] = {nullptr, nullptr};   // HOME moments
+    int cur = 0;
+    float* macro = nullptr;     // 4*N floats: rho, ux, uy, uz (AA; HOME F16/BF16 export)
+    uint8_t* mask = nullptr;    // raw mask as given
+    uint8_t* band = nullptr;
+    uint8_t* flags = nullptr;
+    uint32_t* links = nullptr;
+    int32_t* dist = nullptr;
+    unsigned long long* dcount = nullptr;
+    double* partials = nullptr;
+    double* stats = nullptr;
+    int max_blocks = 0;
+    bool use_flags = false;     // any cell is solid / band / duct boundary
+    bool any_solid = false;
+    bool any_band = false;
+    bool stats_on = false;
+    int last_stat_blocks = 0;
+    int parity = 0;             // AA: 0 natural layout, 1 swapped; reference bounce: 0 A current, 1 B
+    int64_t steps = 0;
+    lbm::LaunchCfg cfg_even{0, 256}, cfg_odd{0, 256};
+    int home_zchunk = 16;
+    // graph cache
+    cudaGraphExec_t gexec = nullptr;
+    int g_sub = 0, g_parity = -1, g_stats = -1;
+};
+
+namespace {
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+            return LBM_ERR_CUDA;                                                   \
+        }                                                                          \
+    } while (0)
+
+bool is_aa(const lbm_solver* s) { return s->method != LBM_METHOD_HOME; }
+// Legacy/Hybrid with the reference's bounce table run the two-buffer push kernel
+bool is_ref_push(const lbm_solver* s) { return is_aa(s) && s->bounce == LBM_BOUNCE_REFERENCE; }
+void* cur_pop(const lbm_solver* s) { return (is_ref_push(s) && s->parity) ? s->f2 : s->f; }
+void* other_pop(const lbm_solver* s) { return (is_ref_push(s) && s->parity) ? s->f : s->f2; }
+
+void drop_graph(lbm_solver* s) {
+    if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
+    s->g_sub = 0; s->g_parity = -1; s->g_stats = -1;
+}
+
+float* home_macro_base(lbm_solver* s) {
+    // F32 HOME exposes its state directly (d_rho() = m + 0*N, home.cu:355-362)
+    return s->storage == LBM_STORE_F32 ? static_cast<float*>(s->m[s->cur]) : s->macro;
+}
+
+int rebuild_flags(lbm_solver* s) {
+    s->use_flags = s->any_solid || s->bc == LBM_BC_DUCT || (s->method == LBM_METHOD_HYBRID && s->any_band);
+    CK(lbm::launch_build_flags(s->any_solid ? s->mask : nullptr,
+                               (s->method == LBM_METHOD_HYBRID && s->any_band) ? s->band : nullptr, s->flags,
+                               s->links, s->dom.nx, s->dom.ny, s->dom.nz, s->bc == LBM_BC_DUCT, s->stream));
+    drop_graph(s);
+    return LBM_OK;
+}
+
+lbm::AAParams aa_params(lbm_solver* s, bool macro, bool stats) {
+    lbm::AAParams p{};
+    p.f = cur_pop(s);
+    p.N = s->N;
+    p.nx = s->dom.nx; p.ny = s->dom.ny; p.nz = s->dom.nz;
+    p.flags = s->use_flags ? s->flags : nullptr;
+    p.links = s->links;
+    p.omega = s->omega;
+    p.omega_h = s->omega;
+    p.omega_s = s->omega_s;
+    p.hybrid = s->method == LBM_METHOD_HYBRID;
+    p.fx = s->dom.force_x; p.fy = s->dom.force_y; p.fz = s->dom.force_z;
+    p.duct = s->bc == LBM_BC_DUCT;
+    p.u_in = s->u_in;
+    p.rho0 = s->rho0;
+    p.rho = s->macro; p.ux = s->macro + s->N; p.uy = s->macro + 2 * s->N; p.uz = s->macro + 3 * s->N;
+    p.macro = macro;
+    p.partials = s->partials;
+    p.stats = stats;
+    return p;
+}
+
+lbm::HomeParams home_params(lbm_solver* s, bool stats) {
+    lbm::HomeParams p{};
+    p.m = s->m[s->cur];
+    p.mn = s->m[s->cur ^ 1];
+    p.N = s->N;
+    p.nx = s->dom.nx; p.ny = s->dom.ny; p.nz = s->dom.nz;
+    p.flags = s->use_flags ? s->flags : nullptr;
+    p.links = s->links;
+    p.omega = s->omega;
+    p.fx = s->dom.force_x; p.fy = s->dom.force_y; p.fz = s->dom.force_z;
+    p.duct = s->bc == LBM_BC_DUCT;
+    p.u_in = s->u_in;
+    p.rho0 = s->rho0;
+    p.partials = s->partials;
+    p.stats = stats;
+    p.zchunk = s->home_zchunk;
+    p.ref_bounce = s->bounce == LBM_BOUNCE_REFERENCE;
+    return p;
+}
+
+}  // namespace
+
+// queue n substeps (no sync)
+static int enqueue_steps(lbm_solver* s, int n) {
+    for (int i = 0; i < n; ++i) {
+        const bool last = (i == n - 1);
+        const bool st = last && s->stats_on;
+        if (is_ref_push(s)) {
+            lbm::AAParams p = aa_params(s, last, st);
+            CK(lbm::launch_ref_push(p, static_cast<const float*>(cur_pop(s)), static_cast<float*>(other_pop(s)),
+                                    s->cfg_odd, s->stream));
+            s->parity ^= 1;
+            if (st) s->last_stat_blocks = s->cfg_odd.blocks;
+        } else if (is_aa(s)) {
+            lbm::AAParams p = aa_params(s, last, st);
+            const lbm::LaunchCfg cfg = s->parity == 0 ? s->cfg_even : s->cfg_odd;
+            CK(lbm::launch_aa_step(p, s->storage, s->parity, cfg, s->stream));
+            s->parity ^= 1;
+            if (st) s->last_stat_blocks = cfg.blocks;
+        } else {
+            lbm::HomeParams p = home_params(s, st);
+            CK(lbm::launch_home_step(p, s->storage, 8, 3, s->stream));
+            s->cur ^= 1;
+            if (st) s->last_stat_blocks = lbm::home_num_blocks(s->dom.nx, s->dom.ny, s->dom.nz, s->home_zchunk);
+        }
+        if (st) CK(lbm::launch_finalize_stats(s->partials, s->last_stat_blocks, s->stats, s->stream));
+    }
+    if (!is_aa(s) && s->storage != LBM_STORE_F32 && n > 0)
+        CK(lbm::launch_home_macros(s->m[s->cur], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
+                                   s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
+    s->steps += n;
+    return LBM_OK;
+}
+
+extern "C" {
+
+const char* lbm_last_error(void) { return lbm::g_error.c_str(); }
+const char* lbm_version(void) { return "lbm_b200 0.1 (sm_100a)"; }
+
+int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out) {
+    if (!dom || !out) { set_error("lbm_create: null argument"); return LBM_ERR_INVALID; }
+    *out = nullptr;
+    if (dom->nx < 1 || dom->ny < 1 || dom->nz < 1) { set_error("lbm_create: dimensions must be >= 1"); return LBM_ERR_INVALID; }
+    if (!(dom->tau > 0.5f)) { set_error("lbm_create: tau must be > 0.5"); return LBM_ERR_INVALID; }
+    lbm_options o{};
+    o.rho0 = 1.0f;
+    if (opts) o = *opts;
+    if (o.method < 0 || o.method > 2) { set_error("lbm_create: bad method"); return LBM_ERR_INVALID; }
+    if (o.storage < 0 || o.storage > 2) { set_error("lbm_create: bad storage"); return LBM_ERR_INVALID; }
+    if (o.bc < 0 || o.bc > 1) { set_error("lbm_create: bad boundary"); return LBM_ERR_INVALID; }
+    if (o.bc == LBM_BC_DUCT && dom->nx < 3) { set_error("lbm_create: a duct needs nx >= 3"); return LBM_ERR_INVALID; }
+    if (o.bounce < 0 || o.bounce > 1) { set_error("lbm_create: bad bounce mode"); return LBM_ERR_INVALID; }
+    if (o.bounce == LBM_BOUNCE_REFERENCE && o.method != LBM_METHOD_HOME && o.storage != LBM_STORE_F32) {
+        set_error("lbm_create: the reference bounce table runs Legacy/Hybrid in F32 storage only");
+        return LBM_ERR_UNSUPPORTED;
+    }
+    const int64_t N = (int64_t)dom->nx * dom->ny * dom->nz;
+    // every population index q*N + id and every plane offset stays in int64;
+    // the per-row x index and the row counts stay in int
+    if (N > ((int64_t)1 << 40) || (int64_t)dom->ny * dom->nz > ((int64_t)1 << 31) - 1) {
+        set_error("lbm_create: grid too large");
+        return LBM_ERR_SIZE;
+    }
+    lbm_solver* s = new lbm_solver();
+    s->dom = *dom;
+    s->method = o.method; s->storage = o.storage; s->bc = o.bc; s->bounce = o.bounce;
+    s->u_in = o.inlet_u;
+    s->rho0 = (o.rho0 > 0.f) ? o.rho0 : 1.0f;
+    s->omega = 1.0f / dom->tau;
+    s->omega_s = s->omega;
+    s->N = N;
+    s->esize = o.storage == LBM_STORE_F32 ? 4 : 2;
+    auto fail = [&](int code) { lbm_destroy(s); return code; };
+    if (o.stream) s->stream = static_cast<cudaStream_t>(o.stream);
+    else {
+        // a blocking stream: ordered with work on the legacy default stream, which
+        // is where the reference's callers (and torch by default) produce inputs
+        if (cudaStreamCreate(&s->stream) != cudaSuccess) {
+            set_error("lbm_create: cudaStreamCreate failed");
+            delete s;
+            return LBM_ERR_CUDA;
+        }
+        s->own_stream = true;
+    }
+    const int sms = lbm::num_sms();
+    s->cfg_even = {sms * 8, 256};
+    s->cfg_odd = {sms * 8, 256};
+    // HOME: enough z-chunks to fill the chip a few times
+    {
+        const int tiles = ((dom->nx + 31) / 32) * ((dom->ny + 7) / 8);
+        int zc = 32;
+        while (zc > 4 && (int64_t)tiles * ((dom->nz + zc - 1) / zc) < (int64_t)sms * 6) zc /= 2;
+        s->home_zchunk = std::min(zc, dom->nz);
+    }
+    s->max_blocks = std::max({s->cfg_even.blocks, s->cfg_odd.blocks,
+                              lbm::home_num_blocks(dom->nx, dom->ny, dom->nz, s->home_zchunk), 1});
+    auto dmalloc = [&](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess; };
+    bool ok = true;
+    if (is_aa(s)) ok = ok && dmalloc(&s->f, s->esize * 19 * (size_t)N);
+    if (is_ref_push(s)) ok = ok && dmalloc(&s->f2, s->esize * 19 * (size_t)N);
+    else ok = ok && dmalloc(&s->m[0], s->esize * 10 * (size_t)N) && dmalloc(&s->m[1], s->esize * 10 * (size_t)N);
+    if (is_aa(s) || s->storage != LBM_STORE_F32) ok = ok && dmalloc((void**)&s->macro, sizeof(float) * 4 * (size_t)N);
+    ok = ok && dmalloc((void**)&s->mask, (size_t)N) && dmalloc((void**)&s->band, (size_t)N) &&
+         dmalloc((void**)&s->flags, (size_t)N) && dmalloc((void**)&s->links, sizeof(uint32_t) * (size_t)N) &&
+         dmalloc((void**)&s->partials, sizeof(double) * lbm::NSTAT * (size_t)s->max_blocks) &&
+         dmalloc((void**)&s->stats, sizeof(double) * lbm::NSTAT) &&
+         dmalloc((void**)&s->dcount, sizeof(unsigned long long));
+    if (!ok) {
+        set_error("lbm_create: device allocation failed (" + std::to_string(N) + " cells)");
+        return fail(LBM_ERR_ALLOC);
+    }
+    if (cudaMemsetAsync(s->mask, 0, (size_t)N, s->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->band, 0, (size_t)N, s->stream) != cudaSuccess ||
+        cudaMemsetAsync(s->stats, 0, sizeof(double) * lbm::NSTAT, s->stream) != cudaSuccess ||
+        (s->f2 && cudaMemsetAsync(s->f2, 0, s->esize * 19 * (size_t)N, s->stream) != cudaSuccess)) {
+        set_error("lbm_create: cudaMemset failed");
+        return fail(LBM_ERR_CUDA);
+    }
+    if (!is_aa(s) && lbm::home_prepare() != cudaSuccess) {
+        set_error("lbm_create: cannot set the HOME kernel's shared-memory size");
+        return fail(LBM_ERR_CUDA);
+    }
+    int rc = rebuild_flags(s);
+    if (rc == LBM_OK) rc = lbm_reset(s);
+    if (rc != LBM_OK) return fail(rc);
+    *out = s;
+    return LBM_OK;
+}
+
+int lbm_destroy(lbm_solver* s) {
+    if (!s) return LBM_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    drop_graph(s);
+    cudaFree(s->f); cudaFree(s->f2); cudaFree(s->m[0]); cudaFree(s->m[1]); cudaFree(s->macro);
+    cudaFree(s->mask); cudaFree(s->band); cudaFree(s->flags); cudaFree(s->links);
+    cudaFree(s->dist); cudaFree(s->dcount); cudaFree(s->partials); cudaFree(s->stats);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return LBM_OK;
+}
+
+int lbm_set_solid_mask(lbm_solver* s, const uint8_t* host_mask) {
+    if (!s || !host_mask) { set_error("lbm_set_solid_mask: null argument"); return LBM_ERR_INVALID; }
+    s->any_solid = false;
+    for (int64_t i = 0; i < s->N; ++i)
+        if (host_mask[i]) { s->any_solid = true; break; }
+    CK(cudaMemcpyAsync(s->mask, host_mask, (size_t)s->N, cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));   // host_mask may be released after return, as in the reference
+    return rebuild_flags(s);
+}
+
+int lbm_set_legacy_mapping(lbm_solver* s, const uint8_t* host_is_legacy) {
+    if (!s) { set_error("lbm_set_legacy_mapping: null solver"); return LBM_ERR_INVALID; }
+    if (s->method != LBM_METHOD_HYBRID) { set_error("lbm_set_legacy_mapping: Hybrid only"); return LBM_ERR_INVALID; }
+    s->any_band = false;
+    if (host_is_legacy) {
+        for (int64_t i = 0; i < s->N; ++i)
+            if (host_is_legacy[i]) { s->any_band = true; break; }
+        CK(cudaMemcpyAsync(s->band, host_is_legacy, (size_t)s->N, cudaMemcpyHostToDevice, s->stream));
+        CK(cudaStreamSynchronize(s->stream));
+    } else {
+        CK(cudaMemsetAsync(s->band, 0, (size_t)s->N, s->stream));
+    }
+    return rebuild_flags(s);
+}
+
+int lbm_build_band(lbm_solver* s, int d0, int64_t* n_band) {
+    if (!s) { set_error("lbm_build_band: null solver"); return LBM_ERR_INVALID; }
+    if (s->method != LBM_METHOD_HYBRID) { set_error("lbm_build_band: Hybrid only"); return LBM_ERR_INVALID; }
+    if (!s->dist && cudaMalloc((void**)&s->dist, sizeof(int32_t) * (size_t)s->N) != cudaSuccess) {
+        set_error("lbm_build_band: allocation failed");
+        return LBM_ERR_ALLOC;
+    }
+    CK(lbm::launch_band(s->mask, s->dist, s->band, s->dom.nx, s->dom.ny, s->dom.nz, d0 < 0 ? 0 : d0, s->dcount,
+                        s->stream));
+    unsigned long long c = 0;
+    CK(cudaMemcpyAsync(&c, s->dcount, sizeof(c), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    s->any_band = c > 0;
+    if (n_band) *n_band = (int64_t)c;
+    return rebuild_flags(s);
+}
+
+int lbm_get_band(lbm_solver* s, uint8_t* out) {
+    if (!s || !out) { set_error("lbm_get_band: null argument"); return LBM_ERR_INVALID; }
+    CK(cudaMemcpyAsync(out, s->band, (size_t)s->N, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return LBM_OK;
+}
+
+int lbm_reset(lbm_solver* s) { return lbm_reinit_from_macro(s, nullptr, nullptr, nullptr, nullptr); }
+
+int lbm_reinit_from_macro(lbm_solver* s, const float* d_rho, const float* d_ux, const float* d_uy,
+                          const float* d_uz) {
+    if (!s) { set_error("lbm_reinit_from_macro: null solver"); return LBM_ERR_INVALID; }
+    if (is_aa(s)) {
+        // Legacy with no rho resets to rho=1, u=0 (legacy.cu:174-178): the same
+        // state as feq(1, 0); Hybrid uses rho=1 and the given u (hybrid.cu:76-79).
+        if (s->method == LBM_METHOD_LEGACY && !d_rho) d_ux = d_uy = d_uz = nullptr;
+        const int form = s->method == LBM_METHOD_LEGACY ? (d_rho ? 0 : 1) : 1;
+        void* dst = cur_pop(s);
+        CK(lbm::launch_aa_reinit(dst, s->storage, s->rho0, s->N, d_rho, d_ux, d_uy, d_uz, s->macro,
+                                 s->macro + s->N, s->macro + 2 * s->N, s->macro + 3 * s->N, form, s->stream));
+        if (is_ref_push(s)) {
+            // the reference's Legacy copies f into fnext after reinitialising
+            // (legacy.cu:204-206); its reset (null rho) and Hybrid's reinit leave
+            // the second buffer as it was
+            if (s->method == LBM_METHOD_LEGACY && d_rho)
+                CK(cudaMemcpyAsync(other_pop(s), dst, s->esize * 19 * (size_t)s->N, cudaMemcpyDeviceToDevice,
+                                   s->stream));
+        } else {
+            s->parity = 0;
+        }
+    } else {
+        CK(lbm::launch_home_reinit(s->m[0], s->m[1], s->storage, s->rho0, s->N, d_rho, d_ux, d_uy, d_uz, s->stream));
+        s->cur = 0;
+        if (s->storage != LBM_STORE_F32)
+            CK(lbm::launch_home_macros(s->m[0], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
+                                       s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
+    }
+    s->steps = 0;
+    drop_graph(s);
+    return LBM_OK;
+}
+
+int lbm_reinit_from_host(lbm_solver* s, const float* rho, const float* ux, const float* uy, const float* uz) {
+    if (!s) { set_error("lbm_reinit_from_host: null solver"); return LBM_ERR_INVALID; }
+    // stage through the solver's own buffers: AA macro fields, or HOME's next buffer
+    float* stage = is_aa(s) ? s->macro : nullptr;
+    float* tmp = nullptr;
+    if (!stage) {
+        if (cudaMallocAsync((void**)&tmp, sizeof(float) * 4 * (size_t)s->N, s->stream) != cudaSuccess) {
+            set_error("lbm_reinit_from_host: allocation failed");
+            return LBM_ERR_ALLOC;
+        }
+        stage = tmp;
+    }
+    const float* src[4] = {rho, ux, uy, uz};
+    const float* dptr[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int k = 0; k < 4; ++k) {
+        if (!src[k]) continue;
+        CK(cudaMemcpyAsync(stage + k * s->N, src[k], sizeof(float) * (size_t)s->N, cudaMemcpyHostToDevice, s->stream));
+        dptr[k] = stage + k * s->N;
+    }
+    const int rc = lbm_reinit_from_macro(s, dptr[0], dptr[1], dptr[2], dptr[3]);
+    if (tmp) cudaFreeAsync(tmp, s->stream);
+    return rc;
+}
+
+int lbm_step(lbm_solver* s, int substeps) {
+    if (!s) { set_error("lbm_step: null solver"); return LBM_ERR_INVALID; }
+    if (substeps < 0) { set_error("lbm_step: negative substeps"); return LBM_ERR_INVALID; }
+    return enqueue_steps(s, substeps);
+}
+
+int lbm_step_graph(lbm_solver* s, int substeps) {
+    if (!s) { set_error("lbm_step_graph: null solver"); return LBM_ERR_INVALID; }
+    if (substeps <= 0) return lbm_step(s, substeps);
+    const int par = is_aa(s) ? s->parity : s->cur;
+    if (!s->gexec || s->g_sub != substeps || s->g_parity != par || s->g_stats != (int)s->stats_on) {
+        drop_graph(s);
+        const int saved_par = s->parity, saved_cur = s->cur;
+        const int64_t saved_steps = s->steps;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue_steps(s, substeps);
+        cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        s->parity = saved_par; s->cur = saved_cur; s->steps = saved_steps;
+        if (rc != LBM_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) { set_error(std::string("graph capture: ") + cudaGetErrorString(e)); return LBM_ERR_CUDA; }
+        e = cudaGraphInstantiate(&s->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { set_error(std::string("graph instantiate: ") + cudaGetErrorString(e)); return LBM_ERR_CUDA; }
+        s->g_sub = substeps; s->g_parity = par; s->g_stats = s->stats_on;
+    }
+    CK(cudaGraphLaunch(s->gexec, s->stream));
+    // advance the host-side state exactly as enqueue_steps would
+    if (is_aa(s)) s->parity ^= (substeps & 1);
+    else s->cur ^= (substeps & 1);
+    s->steps += substeps;
+    return LBM_OK;
+}
+
+int lbm_synchronize(lbm_solver* s) {
+    if (!s) { set_error("lbm_synchronize: null solver"); return LBM_ERR_INVALID; }
+    CK(cudaStreamSynchronize(s->stream));
+    return LBM_OK;
+}
+
+int lbm_set_force(lbm_solver* s, float fx, float fy, float fz) {
+    if (!s) { set_error("lbm_set_force: null solver"); return LBM_ERR_INVALID; }
+    s->dom.force_x = fx; s->dom.force_y = fy; s->dom.force_z = fz;
+    drop_graph(s);
+    return LBM_OK;
+}
+
+int lbm_set_shear_omega(lbm_solver* s, float omega_shear) {
+    if (!s) { set_error("lbm_set_shear_omega: null solver"); return LBM_ERR_INVALID; }
+    if (s->method != LBM_METHOD_HYBRID) { set_error("lbm_set_shear_omega: Hybrid only"); return LBM_ERR_INVALID; }
+    s->omega_s = omega_shear;
+    drop_graph(s);
+    return LBM_OK;
+}
+
+int lbm_macro_ptrs(lbm_solver* s, float** d_rho, float** d_u, float** d_v, float** d_w) {
+    if (!s) { set_error("lbm_macro_ptrs: null solver"); return LBM_ERR_INVALID; }
+    float* b = is_aa(s) ? s->macro : home_macro_base(s);
+    if (d_rho) *d_rho = b;
+    if (d_u) *d_u = b + s->N;
+    if (d_v) *d_v = b + 2 * s->N;
+    if (d_w) *d_w = b + 3 * s->N;
+    return LBM_OK;
+}
+
+int lbm_get_macros(lbm_solver* s, float* rho, float* ux, float* uy, float* uz) {
+    if (!s) { set_error("lbm_get_macros: null solver"); return LBM_ERR_INVALID; }
+    float* b = is_aa(s) ? s->macro : home_macro_base(s);
+    float* dst[4] = {rho, ux, uy, uz};
+    for (int k = 0; k < 4; ++k)
+        if (dst[k]) CK(cudaMemcpyAsync(dst[k], b + k * s->N, sizeof(float) * (size_t)s->N, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return LBM_OK;
+}
+
+int lbm_get_state(lbm_solver* s, float* host_out) {
+    if (!s || !host_out) { set_error("lbm_get_state: null argument"); return LBM_ERR_INVALID; }
+    const int ncomp = is_aa(s) ? 19 : 10;
+    float* tmp = nullptr;
+    CK(cudaMallocAsync((void**)&tmp, sizeof(float) * ncomp * (size_t)s->N, s->stream));
+    cudaError_t e;
+    if (is_aa(s)) {
+        lbm::AAParams p = aa_params(s, false, false);
+        e = lbm::launch_aa_materialize(p, s->storage, is_ref_push(s) ? 0 : s->parity, tmp, s->stream);
+    } else {
+        e = lbm::launch_home_export(s->m[s->cur], s->storage, s->N, s->rho0, tmp, s->stream);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(host_out, tmp, sizeof(float) * ncomp * (size_t)s->N, cudaMemcpyDeviceToHost, s->stream);
+    cudaFreeAsync(tmp, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) { set_error(std::string("lbm_get_state: ") + cudaGetErrorString(e)); return LBM_ERR_CUDA; }
+    return LBM_OK;
+}
+
+int lbm_dims(lbm_solver* s, int32_t* nx, int32_t* ny, int32_t* nz, int64_t* n) {
+    if (!s) { set_error("lbm_dims: null solver"); return LBM_ERR_INVALID; }
+    if (nx) *nx = s->dom.nx;
+    if (ny) *ny = s->dom.ny;
+    if (nz) *nz = s->dom.nz;
+    if (n) *n = s->N;
+    return LBM_OK;
+}
+
+int lbm_step_count(lbm_solver* s, int64_t* steps) {
+    if (!s || !steps) { set_error("lbm_step_count: null argument"); return LBM_ERR_INVALID; }
+    *steps = s->steps;
+    return LBM_OK;
+}
+
+int lbm_enable_stats(lbm_solver* s, int enable) {
+    if (!s) { set_error("lbm_enable_stats: null solver"); return LBM_ERR_INVALID; }
+    s->stats_on = enable != 0;
+    return LBM_OK;
+}
+
+int lbm_get_stats(lbm_solver* s, double* out) {
+    if (!s || !out) { set_error("lbm_get_stats: null argument"); return LBM_ERR_INVALID; }
+    CK(cudaMemcpyAsync(out, s->stats, sizeof(double) * lbm::NSTAT, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return LBM_OK;
+}
+
+int lbm_voxelize(const float* tris, int64_t ntri, const float* bb_in, const lbm_voxel_params* p, uint8_t* mask_out) {
+    if (!p || !mask_out || (ntri > 0 && !tris) || ntri < 0) { set_error("lbm_voxelize: bad argument"); return LBM_ERR_INVALID; }
+    if (p->nx < 1 || p->ny < 1 || p->nz < 1) { set_error("lbm_voxelize: bad dimensions"); return LBM_ERR_INVALID; }
+    const int r = p->refine < 1 ? 1 : p->refine;
+    const int64_t NF = (int64_t)p->nx * r * p->ny * r * p->nz * r;
+    if (NF > ((int64_t)1 << 36)) { set_error("lbm_voxelize: refined grid too large"); return LBM_ERR_SIZE; }
+    float bb[6];
+    if (bb_in) std::memcpy(bb, bb_in, sizeof(bb));
+    else {
+        for (int k = 0; k < 3; ++k) { bb[k] = 3.402823466e+38F; bb[3 + k] = -3.402823466e+38F; }
+        for (int64_t i = 0; i < ntri * 3; ++i)
+            for (int k = 0; k < 3; ++k) {
+                const float v = tris[i * 3 + k];
+                if (v < bb[k]) bb[k] = v;
+                if (bb[3 + k] < v) bb[3 + k] = v;
+            }
+    }
+    const int64_t N = (int64_t)p->nx * p->ny * p->nz;
+    cudaStream_t st = nullptr;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    float* d_tris = nullptr;
+    uint8_t* d_mask = nullptr;
+    cudaError_t e = cudaMallocAsync((void**)&d_tris, sizeof(float) * 9 * (size_t)(ntri > 0 ? ntri : 1), st);
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&d_mask, (size_t)N, st);
+    if (e == cudaSuccess && ntri > 0)
+        e = cudaMemcpyAsync(d_tris, tris, sizeof(float) * 9 * (size_t)ntri, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = lbm::launch_voxelize(d_tris, ntri, bb, p->nx, p->ny, p->nz, p->uniform_scale, p->translate, r,
+                                 p->coverage_threshold, d_mask, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(mask_out, d_mask, (size_t)N, cudaMemcpyDeviceToHost, st);
+    if (d_tris) cudaFreeAsync(d_tris, st);
+    if (d_mask) cudaFreeAsync(d_mask, st);
+    const cudaError_t e2 = cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess) { set_error(std::string("lbm_voxelize: ") + cudaGetErrorString(e)); return LBM_ERR_CUDA; }
+    return LBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,210 @@
+// Shared device definitions for the D3Q19 kernels (sm_100a).
+//
+// Velocity set and weights keep the reference's order so that the population
+// layout f[q*N + id] and the HOME moment layout m[k*N + id] stay the same as
+// the reference's buffers (src/lbm/lbm3d_legacy.cu:16-35,
+// src/lbm/lbm3d_home.hpp:57-71).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "lbm_internal.h"
+
+namespace lbm {
+
+// 0:(0,0,0) 1:(+1,0,0) 2:(-1,0,0) 3:(0,+1,0) 4:(0,-1,0) 5:(0,0,+1) 6:(0,0,-1)
+// 7:(+1,+1,0) 8:(-1,+1,0) 9:(+1,-1,0) 10:(-1,-1,0) 11:(+1,0,+1) 12:(-1,0,+1)
+// 13:(+1,0,-1) 14:(-1,0,-1) 15:(0,+1,+1) 16:(0,-1,+1) 17:(0,+1,-1) 18:(0,-1,-1)
+__host__ __device__ constexpr int cx(int q) {
+    constexpr int t[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
+    return t[q];
+}
+__host__ __device__ constexpr int cy(int q) {
+    constexpr int t[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
+    return t[q];
+}
+__host__ __device__ constexpr int cz(int q) {
+    constexpr int t[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
+    return t[q];
+}
+// the opposite direction, c_opp(q) = -c_q
+__host__ __device__ constexpr int opp(int q) {
+    constexpr int t[19] = {0, 2, 1, 4, 3, 6, 5, 10, 9, 8, 7, 14, 13, 12, 11, 18, 17, 16, 15};
+    return t[q];
+}
+// The reference's opp() table (src/lbm/lbm3d_legacy.cu:29-32): the true
+// opposite for the axis directions, the mirror image in x (xy/xz diagonals)
+// or y (yz diagonals) for the others.  Used only by LBM_BOUNCE_REFERENCE.
+__host__ __device__ constexpr int opp_tab(int q) {
+    constexpr int t[19] = {0, 2, 1, 4, 3, 6, 5, 8, 7, 10, 9, 12, 11, 14, 13, 16, 15, 18, 17};
+    return t[q];
+}
+// weights as the reference writes them: 1.0f/3.0f, 1.0f/18.0f, 1.0f/36.0f
+__host__ __device__ constexpr float wq(int q) {
+    return q == 0 ? 1.0f / 3.0f : (q <= 6 ? 1.0f / 18.0f : 1.0f / 36.0f);
+}
+
+// flag byte per cell, built on the device from the solid mask
+enum : uint8_t {
+    F_SOLID = 1,     // solid cell (frozen populations, macros 1,0,0,0)
+    F_BAND = 2,      // Hybrid: BGK-form collision
+    F_OBST = 4,      // solid cell that counts for the drag (not a wall)
+    F_SPECIAL = 8,   // fluid cell with at least one non-streaming link
+    F_TOUCH = 16,    // fluid cell with a link into an obstacle cell
+};
+
+// The Legacy equilibrium, written as src/lbm/lbm3d_legacy.cu:54-58 writes it
+// (the same expression keeps nvcc's contraction pattern, hence the results, close).
+__device__ __forceinline__ float feq_ref(int q, float rho, float ux, float uy, float uz) {
+    const float eiu = (float)cx(q) * ux + (float)cy(q) * uy + (float)cz(q) * uz;
+    const float uu = ux * ux + uy * uy + uz * uz;
+    return wq(q) * rho * (1.0f + 3.0f * eiu + 4.5f * eiu * eiu - 1.5f * uu);
+}
+
+// ---- storage traits --------------------------------------------------------
+// F32 stores f as is.  F16/BF16 store the shifted value f - w_q*rho0 (all
+// arithmetic stays FP32); the shift keeps the small deviations from the rest
+// state in the narrow mantissa instead of the large constant part.
+struct StoreF32 {
+    using T = float;
+    static constexpr int kId = 0;
+    __device__ __forceinline__ static float ld(const T* p, int q, float r0) { return __ldg(p); }
+    __device__ __forceinline__ static void st(T* p, int q, float r0, float v) { *p = v; }
+    __device__ __forceinline__ static void ld4(const T* p, int q, float r0, float* o) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+    __device__ __forceinline__ static void st4(T* p, int q, float r0, const float* v) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    }
+    __device__ __forceinline__ static void ld2(const T* p, int q, float r0, float* o) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        o[0] = v.x; o[1] = v.y;
+    }
+    __device__ __forceinline__ static void st2(T* p, int q, float r0, const float* v) {
+        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    }
+};
+
+struct StoreF16 {
+    using T = __half;
+    static constexpr int kId = 1;
+    __device__ __forceinline__ static float ld(const T* p, int q, float r0) {
+        return __half2float(*p) + wq(q) * r0;
+    }
+    __device__ __forceinline__ static void st(T* p, int q, float r0, float v) {
+        *p = __float2half_rn(v - wq(q) * r0);
+    }
+    __device__ __forceinline__ static void ld4(const T* p, int q, float r0, float* o) {
+        const uint2 raw = *reinterpret_cast<const uint2*>(p);
+        const __half2 a = *reinterpret_cast<const __half2*>(&raw.x);
+        const __half2 b = *reinterpret_cast<const __half2*>(&raw.y);
+        const float s = wq(q) * r0;
+        const float2 fa = __half22float2(a), fb = __half22float2(b);
+        o[0] = fa.x + s; o[1] = fa.y + s; o[2] = fb.x + s; o[3] = fb.y + s;
+    }
+    __device__ __forceinline__ static void st4(T* p, int q, float r0, const float* v) {
+        const float s = wq(q) * r0;
+        __half2 a = __floats2half2_rn(v[0] - s, v[1] - s);
+        __half2 b = __floats2half2_rn(v[2] - s, v[3] - s);
+        uint2 raw;
+        raw.x = *reinterpret_cast<uint32_t*>(&a);
+        raw.y = *reinterpret_cast<uint32_t*>(&b);
+        *reinterpret_cast<uint2*>(p) = raw;
+    }
+    __device__ __forceinline__ static void ld2(const T* p, int q, float r0, float* o) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(p));
+        const float s = wq(q) * r0;
+        o[0] = f.x + s; o[1] = f.y + s;
+    }
+    __device__ __forceinline__ static void st2(T* p, int q, float r0, const float* v) {
+        const float s = wq(q) * r0;
+        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(v[0] - s, v[1] - s);
+    }
+};
+
+struct StoreBF16 {
+    using T = __nv_bfloat16;
+    static constexpr int kId = 2;
+    __device__ __forceinline__ static float ld(const T* p, int q, float r0) {
+        return __bfloat162float(*p) + wq(q) * r0;
+    }
+    __device__ __forceinline__ static void st(T* p, int q, float r0, float v) {
+        *p = __float2bfloat16_rn(v - wq(q) * r0);
+    }
+    __device__ __forceinline__ static void ld4(const T* p, int q, float r0, float* o) {
+        const uint2 raw = *reinterpret_cast<const uint2*>(p);
+        const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162*>(&raw.x);
+        const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162*>(&raw.y);
+        const float s = wq(q) * r0;
+        const float2 fa = __bfloat1622float2(a), fb = __bfloat1622float2(b);
+        o[0] = fa.x + s; o[1] = fa.y + s; o[2] = fb.x + s; o[3] = fb.y + s;
+    }
+    __device__ __forceinline__ static void st4(T* p, int q, float r0, const float* v) {
+        const float s = wq(q) * r0;
+        __nv_bfloat162 a = __floats2bfloat162_rn(v[0] - s, v[1] - s);
+        __nv_bfloat162 b = __floats2bfloat162_rn(v[2] - s, v[3] - s);
+        uint2 raw;
+        raw.x = *reinterpret_cast<uint32_t*>(&a);
+        raw.y = *reinterpret_cast<uint32_t*>(&b);
+        *reinterpret_cast<uint2*>(p) = raw;
+    }
+    __device__ __forceinline__ static void ld2(const T* p, int q, float r0, float* o) {
+        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+        const float s = wq(q) * r0;
+        o[0] = f.x + s; o[1] = f.y + s;
+    }
+    __device__ __forceinline__ static void st2(T* p, int q, float r0, const float* v) {
+        const float s = wq(q) * r0;
+        *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(v[0] - s, v[1] - s);
+    }
+};
+
+// vector load/store of VEC consecutive cells of one population plane
+template <class ST, int VEC>
+__device__ __forceinline__ void ldv(const typename ST::T* p, int q, float r0, float* o) {
+    if constexpr (VEC == 4) ST::ld4(p, q, r0, o);
+    else if constexpr (VEC == 2) ST::ld2(p, q, r0, o);
+    else o[0] = ST::ld(p, q, r0);
+}
+template <class ST, int VEC>
+__device__ __forceinline__ void stv(typename ST::T* p, int q, float r0, const float* v) {
+    if constexpr (VEC == 4) ST::st4(p, q, r0, v);
+    else if constexpr (VEC == 2) ST::st2(p, q, r0, v);
+    else ST::st(p, q, r0, v[0]);
+}
+
+// ---- FP64 block reduction of NSTAT partial sums ---------------------------
+// Warp shuffles, then one warp over the per-warp results; thread 0 writes the
+// block's NSTAT partials to out[blockIdx.x * NSTAT + k].  Deterministic for a
+// fixed launch shape (a fixed tree per block, a fixed block order in the
+// final pass).
+__device__ __forceinline__ void block_reduce_stats(double (&acc)[NSTAT], double* out) {
+    __shared__ double red[32][NSTAT];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int nwarps = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NSTAT; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NSTAT; ++k) {
+            double v = (lane < nwarps) ? red[lane][k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) out[(size_t)blockIdx.x * NSTAT + k] = v;
+        }
+    }
+    __syncthreads();
+}
+
+}  // namespace lbm

@@ -1,0 +1,99 @@
+// Internal interfaces between the translation units of liblbm_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lbm {
+
+// number of FP64 statistics slots (see LBM_STAT_* in lbm_capi.h)
+constexpr int NSTAT = 8;
+
+// Parameters of one AA-pattern step (Legacy / Hybrid).
+struct AAParams {
+    void* f;                 // 19 planes of N cells, storage type per `storage`
+    int64_t N;
+    int nx, ny, nz;
+    const uint8_t* flags;    // nullptr: no solid cells anywhere
+    const uint32_t* links;   // bit q: link x -> x+c_q does not stream (solid / inlet / outlet)
+    float omega;             // BGK rate (Legacy, and the band cells of Hybrid)
+    float omega_h, omega_s;  // Hybrid non-band cells: fq + wh(feq-fq) + (ws-wh)(-(fq-feq))
+    int hybrid;              // 1: consult F_BAND; 0: BGK form everywhere
+    float fx, fy, fz;
+    int duct;                // 1: x non-periodic with inlet/outlet
+    float u_in;
+    float rho0;              // storage shift reference (F16/BF16)
+    float* rho; float* ux; float* uy; float* uz;   // macro outputs (written when macro != 0)
+    int macro;
+    double* partials;        // [gridDim.x][NSTAT] when stats != 0
+    int stats;
+};
+
+// Parameters of one HOME step (moment-only, two buffers).
+struct HomeParams {
+    const void* m;           // 10 planes [rho,ux,uy,uz,Sxx,Sxy,Sxz,Syy,Syz,Szz]
+    void* mn;
+    int64_t N;
+    int nx, ny, nz;
+    const uint8_t* flags;
+    const uint32_t* links;
+    float omega;
+    float fx, fy, fz;
+    int duct;
+    float u_in;
+    float rho0;
+    double* partials;
+    int stats;
+    int zchunk;              // planes per block
+    int ref_bounce;          // 1: the reference's opposite table for reflections
+};
+
+// Launch configuration chosen by the host (autotuner or defaults).
+struct LaunchCfg {
+    int blocks;
+    int threads;
+};
+
+// AA steps.  parity 0: natural layout in (the even, purely local step);
+// parity 1: the odd step (gathers from and scatters to neighbours).
+cudaError_t launch_aa_step(const AAParams& p, int storage, int parity, LaunchCfg cfg, cudaStream_t s);
+// Reference-compatible Legacy/Hybrid step (two buffers, the reference's
+// opposite table): fa -> fb.
+cudaError_t launch_ref_push(const AAParams& p, const float* fa, float* fb, LaunchCfg cfg, cudaStream_t s);
+// Copies the populations into the reference's natural layout (float, 19*N)
+// whatever the parity, without advancing.
+cudaError_t launch_aa_materialize(const AAParams& p, int storage, int parity, float* out, cudaStream_t s);
+// sets the dynamic shared-memory limit of the HOME kernels (call outside graph capture)
+cudaError_t home_prepare();
+int home_num_blocks(int nx, int ny, int nz, int zchunk);
+cudaError_t launch_home_step(const HomeParams& p, int storage, int tile_y, int blocks_per_sm, cudaStream_t s);
+// HOME moments (storage type) -> float 10*N
+cudaError_t launch_home_export(const void* m, int storage, int64_t N, float rho0, float* out, cudaStream_t s);
+// macro pointers of a HOME state in F16/BF16 are exported to float buffers
+cudaError_t launch_home_macros(const void* m, int storage, int64_t N, float rho0,
+                               float* rho, float* ux, float* uy, float* uz, cudaStream_t s);
+
+// initialisation
+cudaError_t launch_aa_reinit(void* f, int storage, float rho0, int64_t N,
+                             const float* rho, const float* ux, const float* uy, const float* uz,
+                             float* rho_out, float* ux_out, float* uy_out, float* uz_out,
+                             int feq_form, cudaStream_t s);
+cudaError_t launch_home_reinit(void* m, void* mn, int storage, float rho0, int64_t N,
+                               const float* rho, const float* ux, const float* uy, const float* uz,
+                               cudaStream_t s);
+
+// flags / links / band
+cudaError_t launch_build_flags(const uint8_t* mask, const uint8_t* band, uint8_t* flags, uint32_t* links,
+                               int nx, int ny, int nz, int duct, cudaStream_t s);
+cudaError_t launch_band(const uint8_t* mask, int32_t* dist, uint8_t* band, int nx, int ny, int nz, int d0,
+                        unsigned long long* count, cudaStream_t s);
+cudaError_t launch_finalize_stats(const double* partials, int nblocks, double* out, cudaStream_t s);
+
+// geometry
+cudaError_t launch_voxelize(const float* d_tris, int64_t ntri, const float* bb, int nx, int ny, int nz,
+                            float scale, const float* translate, int refine, float thr, uint8_t* d_mask,
+                            cudaStream_t s);
+
+int num_sms();
+
+}  // namespace lbm

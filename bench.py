@@ -1,0 +1,441 @@
+#!/usr/bin/env python
+"""D3Q19 MLUPS and HBM-roofline fraction on the duct-past-a-sphere workload.
+
+Workload (one bench step = one drag interval): a 256x128x128 duct, velocity
+inlet u=0.05 at x=0, zero-gradient outlet, halfway bounce-back walls on the
+y/z faces, tau=0.56, flow past an icosphere (5,120 triangles, radius 16
+cells, centre (64,64,64)) voxelized on the GPU; 50 LBM steps with the
+momentum-exchange drag recorded at the last one.  Inputs are synthetic
+(generated from fixed parameters; no dataset).  The state (319 MB of FP32
+populations) is larger than L2, so no flush is needed between steps.
+
+`value` is Legacy BGK FP32 (the fluidsim_legacy path); HOME and Hybrid(B0=2)
+are measured on the same workload and reported under "methods".
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With --gpus N (under torchrun) every rank runs its own duct instance (weak
+scaling, no data-path collective); time is the max over ranks.
+--impl reference times the reference's own CUDA build (compiled from its
+sources into oracle/_ref) on the closest workload it supports: the same grid,
+mask and tau with the duct walls as solid cells, periodic in x and driven by
+a body force, because the reference has no inlet/outlet boundary.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX, NY, NZ = 256, 128, 128
+TAU = 0.56
+U_IN = 0.05
+DRAG_EVERY = 50
+RADIUS, CENTER = 16, (64, 64, 64)
+B0 = 2
+# algorithmic bytes per cell-update (state read once + written once, plus the mask/flag byte)
+BYTES = {"legacy": 19 * 4 * 2 + 1, "hybrid": 19 * 4 * 2 + 1, "home": 10 * 4 * 2 + 1}
+KERNEL = {"legacy": "aa_even/aa_odd", "hybrid": "aa_even/aa_odd", "home": "home_step"}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(method):
+    """DRAM bytes per cell of the dominant kernel from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        m = re.match(r"\|\s*%s\s*\|\s*([0-9.]+)\s*\|" % method, line)
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def build_mask(tmpdir):
+    """Icosphere STL -> library loader -> GPU voxelizer -> duct walls."""
+    from myfluidsimulation_b200 import geometry as G
+    from myfluidsimulation_b200 import workloads as W
+    tris, scale, tr = W.duct_sphere_mesh(NX, NY, NZ, RADIUS, CENTER)
+    path = os.path.join(tmpdir, "icosphere.stl")
+    W.write_binary_stl(path, tris)
+    mesh = G.load_stl(path)
+    sphere = G.voxelize_mesh_to_mask(mesh, G.VoxelParams(NX, NY, NZ, scale, tr))
+    return W.duct_mask(NX, NY, NZ, sphere), int(mesh.tris.shape[0]), int(sphere.sum())
+
+
+def make_solver(method, mask, stream):
+    from myfluidsimulation_b200.solvers import BC_DUCT, METHOD_HOME, METHOD_HYBRID, METHOD_LEGACY, Solver
+    m = {"legacy": METHOD_LEGACY, "home": METHOD_HOME, "hybrid": METHOD_HYBRID}[method]
+    s = Solver(NX, NY, NZ, TAU, method=m, bc=BC_DUCT, inlet_u=U_IN, stream=stream)
+    s.set_solid_mask(mask)
+    nb = s.build_band(B0) if method == "hybrid" else 0
+    rho = np.ones((NZ, NY, NX), np.float32)
+    u = np.full((NZ, NY, NX), U_IN, np.float32)
+    u[mask != 0] = 0
+    s.reinit_from_host(rho, u, None, None)
+    s.enable_stats(True)
+    return s, nb
+
+
+def run_method(method, mask, args, torch, rank):
+    st = torch.cuda.current_stream()
+    s, nb = make_solver(method, mask, st.cuda_stream)
+    for _ in range(args.warmup):
+        s.step(DRAG_EVERY)
+    torch.cuda.synchronize()
+    drags = []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        s.step(DRAG_EVERY)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    st_ = s.stats()
+    drags.append([st_["drag_x"], st_["drag_y"], st_["drag_z"]])
+    res = {"ms_total": ms, "launches": args.steps * (DRAG_EVERY + 1), "band_cells": nb,
+           "drag_last": drags[-1], "mass": st_["mass"]}
+    # per-kernel split (outside the timed region): single steps, no macro/stats output,
+    # CUDA events around each launch; Legacy/Hybrid alternate the even and odd kernels
+    s.enable_stats(False)
+    s.set_macro_output(False)
+    split = [[], []]
+    for i in range(20):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        s.step(1)
+        b.record(st)
+        torch.cuda.synchronize()
+        split[i % 2].append(a.elapsed_time(b))
+    s.set_macro_output(True)
+    s.enable_stats(True)
+    par = (args.warmup + args.steps) * DRAG_EVERY % 2      # parity of the first split launch
+    if method == "home":
+        res["kernel_us"] = {"home_step": round(1e3 * statistics.median(split[0] + split[1]), 2)}
+    else:
+        names = ("aa_even", "aa_odd") if par == 0 else ("aa_odd", "aa_even")
+        res["kernel_us"] = {names[0]: round(1e3 * statistics.median(split[0]), 2),
+                            names[1]: round(1e3 * statistics.median(split[1]), 2)}
+    return s, res
+
+
+def e2e_run(method, mask, args, torch):
+    """Through the public API with host buffers: each step uploads the macro fields
+    from pinned host memory (reinit), runs one drag interval and reads the macro
+    fields and the statistics back."""
+    st = torch.cuda.current_stream()
+    s, _ = make_solver(method, mask, st.cuda_stream)
+    N = NX * NY * NZ
+    pin = lambda: torch.empty(N, dtype=torch.float32, pin_memory=True).numpy().reshape(NZ, NY, NX)
+    rho_h, u_h, v_h, w_h = pin(), pin(), pin(), pin()
+    rho_h[:] = 1.0
+    u_h[:] = U_IN
+    u_h[mask != 0] = 0
+    v_h[:] = 0
+    w_h[:] = 0
+    outs = [pin() for _ in range(4)]
+    import ctypes as C
+    from myfluidsimulation_b200._lib import check, lib
+    L = lib()
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    stats = np.zeros(8, np.float64)
+
+    def one():
+        check(L.lbm_reinit_from_host(s._h, vp(rho_h), vp(u_h), vp(v_h), vp(w_h)))
+        check(L.lbm_step(s._h, DRAG_EVERY))
+        check(L.lbm_get_macros(s._h, *[vp(o) for o in outs]))
+        check(L.lbm_get_stats(s._h, vp(stats)))
+
+    for _ in range(max(1, args.warmup // 2)):
+        one()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(args.steps):
+        one()
+    e1.record(st)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) * 1e3
+    ms = max(e0.elapsed_time(e1), 0.0)
+    s.close()
+    return ms, wall, 4 * 4 * N, 4 * 4 * N + 8 * 8
+
+
+def cpu_baseline(mask, gpu_state_fn):
+    """The FP64 oracle (the C restatement, OpenMP over the host cores) on a bounded
+    sample of the same workload: the full grid for a few steps."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_bind import Oracle
+    o = Oracle()
+    nthreads = o.lib.orc_num_threads()
+    rho = np.ones((NZ, NY, NX))
+    u = np.full((NZ, NY, NX), np.float64(np.float32(U_IN)))
+    u[mask != 0] = 0
+    f0 = o.reinit_eq(rho, u, None, None)
+    # size the sample to ~10-20 s: time one step first
+    t = time.perf_counter()
+    o.bgk_run(f0, mask, 1, TAU, bc=1, u_in=np.float32(U_IN))
+    t1 = time.perf_counter() - t
+    steps = int(max(2, min(40, 12.0 / max(t1, 1e-3))))
+    t = time.perf_counter()
+    f, r, ux, uy, uz, drag = o.bgk_run(f0, mask, steps, TAU, bc=1, u_in=np.float32(U_IN))
+    dt = time.perf_counter() - t
+    mlups = NX * NY * NZ * steps / dt / 1e6
+    # the same sample on the GPU: relative L2 of the state against FP64
+    g = gpu_state_fn(steps)
+    err = float(np.linalg.norm(g - f) / np.linalg.norm(f))
+    return {"value": round(mlups, 2), "unit": "MLUPS", "cores": int(nthreads), "kind": "port",
+            "sample": f"FP64 oracle (C, OpenMP) Legacy BGK duct {NX}x{NY}x{NZ}, {steps} steps"}, err, steps
+
+
+def reference_arm(args, torch, rank, world):
+    """The reference's own CUDA build on the same grid/mask/tau, force-driven periodic duct."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_bind import RefCUDA
+    base = {"metric": "D3Q19 MLUPS (Legacy BGK FP32, duct 256x128x128 past a voxelized sphere)", "unit": "MLUPS",
+            "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+    if not RefCUDA.available():
+        if rank == 0:
+            base.update({"unavailable": "reference CUDA build oracle/_ref/libref_cuda.so not present"})
+            print(json.dumps(base))
+        return
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as td:
+        mask, ntri, nsph = build_mask(td)
+    R = RefCUDA()
+    h = R.create(0, (NX, NY, NZ), TAU, (1e-5, 0.0, 0.0))
+    R.set_mask(h, (mask != 0).astype(np.uint8))
+    R.init_rho(h, None)
+    R.time_steps(h, args.warmup, DRAG_EVERY)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        ms = R.time_steps(h, args.steps, DRAG_EVERY)
+    R.destroy(h)
+    N = NX * NY * NZ
+    mlups = N * DRAG_EVERY * args.steps / (ms * 1e-3) / 1e6
+    base.update({
+        "value": round(mlups, 1), "ms_per_step": round(ms / args.steps, 4),
+        "config": {"workload": "duct 256x128x128, icosphere r=16 mask, tau 0.56, walls as solid cells, "
+                               "x periodic, body force 1e-5 (the reference has no inlet/outlet)",
+                   "method": "LBM3D_Legacy::step(50) of the reference build", "l2": "state 637 MB > L2"},
+        "cpu_baseline": {"value": round(mlups, 1), "unit": "MLUPS", "cores": 0, "kind": "reference",
+                         "device": "cuda:0",
+                         "sample": f"reference CUDA build (oracle/_ref/libref_cuda.so), {args.steps}x50 steps"},
+        "e2e": {"value": round(mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk.summary(),
+    })
+    print(json.dumps(base))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--methods", default="legacy,home,hybrid")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", default=None,
+                    help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    if args.impl == "reference":
+        reference_arm(args, torch, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import myfluidsimulation_b200 as P
+    P.lib()
+    with tempfile.TemporaryDirectory() as td:
+        mask, ntri, nsph = build_mask(td)
+    if args.profile:
+        st = torch.cuda.current_stream()
+        s, _ = make_solver(args.profile, mask, st.cuda_stream)
+        s.enable_stats(False)
+        for _ in range(4):
+            s.step(1)
+        s.synchronize()
+        s.close()
+        print(json.dumps({"profile": args.profile, "steps": 4}))
+        return
+    methods = [m for m in args.methods.split(",") if m]
+    peak, peak_kind = measured_peaks()
+    N = NX * NY * NZ
+    results = {}
+    clocks = None
+    head = methods[0]
+    clk = ClockSampler(local).__enter__()   # spans the timed regions of all methods
+    for mth in methods:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        s, r = run_method(mth, mask, args, torch, rank)
+        ms = torch.tensor([r["ms_total"]], device="cuda")
+        if dist:
+            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        ms = float(ms.item())
+        cell_updates = N * DRAG_EVERY * args.steps * world
+        mlups = cell_updates / (ms * 1e-3) / 1e6
+        per_launch_ms = r["ms_total"] / (DRAG_EVERY * args.steps)
+        achieved = N * BYTES[mth] / (per_launch_ms * 1e-3) / 1e9
+        tr = profile_traffic(mth)
+        results[mth] = {"mlups": round(mlups, 1), "ms_per_step": round(ms / args.steps, 4),
+                        "kernel_us": r["kernel_us"],
+                        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                                     "frac": round(achieved / peak, 4),
+                                     "traffic": None if tr is None else round(tr * N / 1e6, 2),
+                                     "kernel": KERNEL[mth], "bytes_per_cell": BYTES[mth]},
+                        "drag": [round(x, 6) for x in r["drag_last"]], "mass": round(r["mass"], 3),
+                        "launches": r["launches"]}
+        if mth == "hybrid":
+            results[mth]["band_cells"] = r["band_cells"]
+        if mth == head:
+            head_solver = s
+        else:
+            s.close()
+
+    clk.__exit__()
+    clocks = clk.summary()
+    # end to end through the C-ABI with host buffers (headline method)
+    e2e_ms, e2e_wall, h2d, d2h = e2e_run(head, mask, args, torch)
+    e2e_t = torch.tensor([e2e_ms], device="cuda")
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_mlups = N * DRAG_EVERY * args.steps * world / (float(e2e_t.item()) * 1e-3) / 1e6
+
+    cpu = None
+    l2 = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        def gpu_state(steps):
+            st = torch.cuda.current_stream()
+            g, _ = make_solver(head, mask, st.cuda_stream)
+            g.enable_stats(False)
+            g.step(steps)
+            g.synchronize()
+            out = g.state()
+            g.close()
+            return out
+        try:
+            cpu, l2, l2_steps = cpu_baseline(mask, gpu_state)
+        except Exception as e:  # the checker is optional on a box without it
+            cpu = {"value": None, "unavailable": f"{type(e).__name__}: {e}"}
+    head_solver.close()
+
+    if rank == 0:
+        h = results[head]
+        line = {
+            "metric": "D3Q19 MLUPS (Legacy BGK FP32, duct 256x128x128 past a voxelized sphere)",
+            "value": h["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": h["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "duct 256x128x128, inlet u=0.05, outflow, y/z walls, icosphere "
+                                   f"({ntri} triangles, r=16, {nsph} solid cells) voxelized on the GPU, tau 0.56; "
+                                   "one step = 50 LBM steps + drag",
+                       "method": head, "storage": "f32", "bounce": "halfway (AA in-place)",
+                       "l2": "inputs larger than L2 (319 MB FP32 state)", "parallelism": f"replicas x{world}"},
+            "roofline": dict(h["roofline"], peak_kind=peak_kind),
+            "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "wall_ms": round(e2e_wall, 2)},
+            "gpu_launches": sum(r["launches"] for r in results.values()),
+            "methods": results,
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        if l2 is not None:
+            line["l2_vs_fp64"] = {"value": l2, "what": f"relative L2 of the {head} state vs the FP64 oracle",
+                                  "steps": l2_steps}
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

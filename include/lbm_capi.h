@@ -177,6 +177,13 @@ int lbm_enable_stats(lbm_solver* s, int enable);
  * src/bench/main_taylor_green.cpp:157-182). */
 int lbm_get_stats(lbm_solver* s, double* out);
 
+/* Enables (1, the default) or disables (0) the macro-field output of
+ * Legacy/Hybrid steps.  Disabled, lbm_step writes only the populations (the
+ * macro buffers keep their last values), which saves 16 B per cell on the
+ * last substep; statistics, when enabled, still write them.  HOME's macro
+ * fields are its state and are always current. */
+int lbm_set_macro_output(lbm_solver* s, int enable);
+
 /* Captures `substeps` steps into a CUDA graph on first use and replays it;
  * same result as lbm_step.  Invalidated by any setter. */
 int lbm_step_graph(lbm_solver* s, int substeps);

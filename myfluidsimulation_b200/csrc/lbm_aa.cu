@@ -14,9 +14,11 @@
 // A link x -> x+c_q that does not stream (solid target, or the duct's inlet /
 // outlet planes) sends its value back into the cell's own slot opp(q), where
 // the next odd step's gather (or the next even step's natural read) picks it up:
-//   solid target : f*_q                      (halfway bounce-back, legacy.cu:100-104)
-//   inlet (x<0)  : feq_opp(q)(rho, u_in)
+//   solid target : f*_q                      (halfway bounce-back)
+//   inlet (x<0)  : feq_opp(q)(rho, (u_in,0,0)) = w_q rho (1 + 3 u_in + 3 u_in^2)
 //   outlet (x>=Nx): f*_opp(q)
+// Link handling is branch-free: per direction the address and the value are
+// selected, so a warp holding one boundary cell does not run a second path.
 // Macro outputs are the moments of the populations the step starts from, as the
 // reference's kernels write them before colliding (legacy.cu:78-90,110-113).
 #include "lbm_common.cuh"
@@ -29,59 +31,71 @@ struct Cell {
     float r, ux, uy, uz;
 };
 
-// Pre-collision moments with the velocity-shift force (legacy.cu:78-90).  The
-// sums run in the reference's q order; the +-1 components add or subtract.
+// Pre-collision moments with the velocity-shift force (legacy.cu:78-90).
+// Opposite pairs are summed first: s = f_q + f_opp, d = f_q - f_opp.
 __device__ __forceinline__ Cell moments(const float (&f)[19], float fx, float fy, float fz) {
-    float r = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-    for (int q = 0; q < 19; ++q) {
-        r += f[q];
-        if (cx(q) > 0) jx += f[q]; else if (cx(q) < 0) jx -= f[q];
-        if (cy(q) > 0) jy += f[q]; else if (cy(q) < 0) jy -= f[q];
-        if (cz(q) > 0) jz += f[q]; else if (cz(q) < 0) jz -= f[q];
-    }
+    // pairs with their positive member: (1,2) x, (3,4) y, (5,6) z, (7,10) +x+y,
+    // (9,8) +x-y, (11,14) +x+z, (13,12) +x-z, (15,18) +y+z, (17,16) +y-z
+    const float s12 = f[1] + f[2], d12 = f[1] - f[2];
+    const float s34 = f[3] + f[4], d34 = f[3] - f[4];
+    const float s56 = f[5] + f[6], d56 = f[5] - f[6];
+    const float s7 = f[7] + f[10], d7 = f[7] - f[10];
+    const float s9 = f[9] + f[8], d9 = f[9] - f[8];
+    const float s11 = f[11] + f[14], d11 = f[11] - f[14];
+    const float s13 = f[13] + f[12], d13 = f[13] - f[12];
+    const float s15 = f[15] + f[18], d15 = f[15] - f[18];
+    const float s17 = f[17] + f[16], d17 = f[17] - f[16];
     Cell c;
-    c.r = r;
-    c.ux = ((r > 0.f) ? jx / r : 0.f) + fx;
-    c.uy = ((r > 0.f) ? jy / r : 0.f) + fy;
-    c.uz = ((r > 0.f) ? jz / r : 0.f) + fz;
+    c.r = f[0] + ((s12 + s34) + (s56 + s7)) + ((s9 + s11) + (s13 + s15) + s17);
+    const float jx = (d12 + d7) + (d9 + d11) + d13;
+    const float jy = (d34 + d7) - d9 + (d15 + d17);
+    const float jz = (d56 + d11) - d13 + (d15 - d17);
+    const float inv = c.r > 0.f ? 1.0f / c.r : 0.f;
+    c.ux = jx * inv + fx;
+    c.uy = jy * inv + fy;
+    c.uz = jz * inv + fz;
     return c;
 }
 
-// Post-collision populations.  Band (or Legacy) cells: fq + w(feq - fq)
-// (legacy.cu:92-95); Hybrid non-band cells: the algebraic "HOME form" of
-// hybrid.cu:148-152, identical to BGK when omega_s == omega_h.
-__device__ __forceinline__ void collide(const float (&f)[19], float (&o)[19], const Cell& c,
-                                        bool bgk_form, float omega, float omega_h, float omega_s) {
-#pragma unroll
-    for (int q = 0; q < 19; ++q) {
-        const float fe = feq_ref(q, c.r, c.ux, c.uy, c.uz);
-        const float fq = f[q];
-        if (bgk_form) {
-            o[q] = fq + omega * (fe - fq);
-        } else {
-            const float ds = fq - fe;
-            o[q] = fq + omega_h * (fe - fq) + (omega_s - omega_h) * (-ds);
-        }
-    }
+// BGK collision f* = f + w (feq - f) for every direction, the equilibrium
+// evaluated per opposite pair: feq_(+-) = w rho (1 - 1.5u^2 + 4.5 t^2) +- 3 w rho t.
+// (The Hybrid's "HOME form" of hybrid.cu:148-152 is this with w = omega_shear.)
+__device__ __forceinline__ void collide(float (&f)[19], const Cell& c, float omega) {
+    const float A = 1.0f - 1.5f * (c.ux * c.ux + c.uy * c.uy + c.uz * c.uz);
+    const float r0 = (1.0f / 3.0f) * c.r, r1 = (1.0f / 18.0f) * c.r, r2 = (1.0f / 36.0f) * c.r;
+    auto pair = [&](int qp, int qm, float t, float wr) {
+        const float sym = wr * fmaf(4.5f * t, t, A);
+        const float asym = 3.0f * wr * t;
+        f[qp] = fmaf(omega, (sym + asym) - f[qp], f[qp]);
+        f[qm] = fmaf(omega, (sym - asym) - f[qm], f[qm]);
+    };
+    f[0] = fmaf(omega, r0 * A - f[0], f[0]);
+    pair(1, 2, c.ux, r1);
+    pair(3, 4, c.uy, r1);
+    pair(5, 6, c.uz, r1);
+    pair(7, 10, c.ux + c.uy, r2);
+    pair(9, 8, c.ux - c.uy, r2);
+    pair(11, 14, c.ux + c.uz, r2);
+    pair(13, 12, c.ux - c.uz, r2);
+    pair(15, 18, c.uy + c.uz, r2);
+    pair(17, 16, c.uy - c.uz, r2);
 }
 
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 // Momentum exchanged with obstacle cells along the solid links of one cell.
-__device__ __forceinline__ void add_drag(double (&acc)[NSTAT], const float (&o)[19], uint32_t lk,
-                                         const uint8_t* flags, int x, int y, int z, int nx, int ny, int nz,
-                                         int duct) {
-#pragma unroll
+__device__ __noinline__ void add_drag(double* acc, const float* o, uint32_t lk, const uint8_t* flags, int x, int y,
+                                      int z, int nx, int ny, int nz, int duct) {
     for (int q = 1; q < 19; ++q) {
         if (!((lk >> q) & 1u)) continue;
-        const int xt = x + cx(q);
+        const int ex = cx(q), ey = cy(q), ez = cz(q);
+        const int xt = x + ex;
         if (duct && (xt < 0 || xt >= nx)) continue;
-        const int64_t t = ((int64_t)wrap(z + cz(q), nz) * ny + wrap(y + cy(q), ny)) * nx + wrap(xt, nx);
+        const int64_t t = ((int64_t)wrap(z + ez, nz) * ny + wrap(y + ey, ny)) * nx + wrap(xt, nx);
         if (flags[t] & F_OBST) {
-            acc[2] += 2.0 * cx(q) * (double)o[q];
-            acc[3] += 2.0 * cy(q) * (double)o[q];
-            acc[4] += 2.0 * cz(q) * (double)o[q];
+            acc[2] += 2.0 * ex * (double)o[q];
+            acc[3] += 2.0 * ey * (double)o[q];
+            acc[4] += 2.0 * ez * (double)o[q];
         }
     }
 }
@@ -94,28 +108,32 @@ __device__ __forceinline__ void add_cell_stats(double (&acc)[NSTAT], const Cell&
     acc[7] += (double)c.r * c.uz;
 }
 
+// Inlet replacement for the incoming direction opp(q): the equilibrium at
+// (rho, (u_in,0,0)) of a direction with c_x = +1 is w rho (1 + 3u + 3u^2);
+// `kin` = 1 + 3u + 3u^2.
+__device__ __forceinline__ float inlet_value(int q, float r, float kin) { return wq(q) * r * kin; }
+
 // ---------------------------------------------------------------------------
-// Even step: local.  VEC consecutive cells per thread (VEC=4: one 16-byte
-// (F32) or 8-byte (F16/BF16) access per population and thread).
-// ---------------------------------------------------------------------------
+// Even step: local.  VEC consecutive cells per thread.
 // MODE 0: populations only; 1: + macro fields; 2: + macro fields + statistics
-template <class ST, bool MASK, int VEC, int MODE>
+// ---------------------------------------------------------------------------
+template <class ST, bool MASK, int VEC, int MODE, class IDX>
 __global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     using T = typename ST::T;
     T* __restrict__ f = static_cast<T*>(p.f);
-    const int64_t N = p.N;
-    const int64_t nvec = N / VEC;
+    const IDX N = (IDX)p.N;
+    const IDX nvec = N / VEC;
+    const float kin = 1.0f + 3.0f * p.u_in + 3.0f * p.u_in * p.u_in;
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
 
-    for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvec;
-         v += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t id = v * VEC;
+    for (IDX v = (IDX)blockIdx.x * blockDim.x + threadIdx.x; v < nvec; v += (IDX)gridDim.x * blockDim.x) {
+        const IDX id = v * VEC;
         float a[19][VEC];
 #pragma unroll
-        for (int q = 0; q < 19; ++q) ldv<ST, VEC>(f + q * N + id, q, p.rho0, a[q]);
+        for (int q = 0; q < 19; ++q) ldv<ST, VEC>(f + (IDX)q * N + id, q, p.rho0, a[q]);
         uint32_t fl4 = 0;
         if constexpr (MASK) {
             if constexpr (VEC == 4) fl4 = *reinterpret_cast<const uint32_t*>(p.flags + id);
@@ -123,7 +141,7 @@ __global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
             else fl4 = p.flags[id];
         }
         int x0 = 0;
-        if (p.duct) x0 = (int)(id % p.nx);
+        if (p.duct) x0 = (int)(id % (IDX)p.nx);
         float mr[VEC], mu[VEC], mv[VEC], mw[VEC];
 #pragma unroll
         for (int l = 0; l < VEC; ++l) {
@@ -131,45 +149,40 @@ __global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
             float c[19];
 #pragma unroll
             for (int q = 0; q < 19; ++q) c[q] = a[q][l];
-            if (MASK && (fl & F_SOLID)) {
-                // frozen (legacy.cu:72-76): slot opp(q) gets its own value back
-#pragma unroll
-                for (int q = 0; q < 19; ++q) a[q][l] = c[opp(q)];
-                mr[l] = 1.f; mu[l] = mv[l] = mw[l] = 0.f;
-                continue;
-            }
             const Cell m = moments(c, p.fx, p.fy, p.fz);
+            const bool solid = MASK && (fl & F_SOLID);
+            const float om = (p.hybrid && !(fl & F_BAND)) ? p.omega_s : p.omega;
             float o[19];
-            const bool bgk = !p.hybrid || (fl & F_BAND);
-            collide(c, o, m, bgk, p.omega, p.omega_h, p.omega_s);
-            if (STATS) {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) o[q] = c[q];
+            collide(o, m, om);
+            if (STATS && !solid) {
                 add_cell_stats(acc, m);
                 if (MASK && (fl & F_TOUCH)) {
-                    const int64_t x = id + l;
-                    const int xi = (int)(x % p.nx);
-                    const int64_t row = x / p.nx;
-                    add_drag(acc, o, p.links[id + l], p.flags, xi, (int)(row % p.ny), (int)(row / p.ny),
+                    const IDX xg = id + l;
+                    const int xi = (int)(xg % (IDX)p.nx);
+                    const IDX row = xg / (IDX)p.nx;
+                    add_drag(acc, o, p.links[xg], p.flags, xi, (int)(row % (IDX)p.ny), (int)(row / (IDX)p.ny),
                              p.nx, p.ny, p.nz, p.duct);
                 }
             }
-            if (p.duct) {
-                const int x = x0 + l;
-                if (x == 0) {
+            const int x = x0 + l;
+            const bool at_in = p.duct && x == 0, at_out = p.duct && x == p.nx - 1;
 #pragma unroll
-                    for (int q = 0; q < 19; ++q)
-                        if (cx(q) < 0) o[q] = feq_ref(opp(q), m.r, p.u_in, 0.f, 0.f);
-                } else if (x == p.nx - 1) {
-#pragma unroll
-                    for (int q = 0; q < 19; ++q)
-                        if (cx(q) > 0) o[q] = o[opp(q)];
-                }
+            for (int q = 0; q < 19; ++q) {
+                float v = o[q];
+                if (cx(q) < 0) v = at_in ? inlet_value(q, m.r, kin) : v;
+                if (cx(q) > 0) v = at_out ? o[opp(q)] : v;
+                // a solid cell keeps its populations (legacy.cu:72-76): slot opp(q) gets its own value
+                a[q][l] = solid ? c[opp(q)] : v;
             }
-#pragma unroll
-            for (int q = 0; q < 19; ++q) a[q][l] = o[q];
-            mr[l] = m.r; mu[l] = m.ux; mv[l] = m.uy; mw[l] = m.uz;
+            mr[l] = solid ? 1.f : m.r;
+            mu[l] = solid ? 0.f : m.ux;
+            mv[l] = solid ? 0.f : m.uy;
+            mw[l] = solid ? 0.f : m.uz;
         }
 #pragma unroll
-        for (int q = 0; q < 19; ++q) stv<ST, VEC>(f + opp(q) * N + id, q, p.rho0, a[q]);
+        for (int q = 0; q < 19; ++q) stv<ST, VEC>(f + (IDX)opp(q) * N + id, q, p.rho0, a[q]);
         if constexpr (MACRO) {
             stv<StoreF32, VEC>(p.rho + id, 0, 0.f, mr);
             stv<StoreF32, VEC>(p.ux + id, 0, 0.f, mu);
@@ -183,9 +196,10 @@ __global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
 // Neighbour addressing of one cell: 9 row bases (dy,dz in -1..1, periodic in
 // y and z) and 3 x positions (periodic in x; in a duct the out-of-range ones
 // are never used because those links are marked as not streaming).
+template <class IDX>
 struct Nbr {
-    int64_t r[3][3];   // [dy+1][dz+1]
-    int xs[3];         // [dx+1]
+    IDX r[3][3];   // [dy+1][dz+1]
+    int xs[3];     // [dx+1]
     __device__ __forceinline__ void init(int x, int y, int z, int nx, int ny, int nz) {
         const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
         const int zm = z == 0 ? nz - 1 : z - 1, zp = z == nz - 1 ? 0 : z + 1;
@@ -194,71 +208,72 @@ struct Nbr {
 #pragma unroll
         for (int a = 0; a < 3; ++a)
 #pragma unroll
-            for (int b = 0; b < 3; ++b) r[a][b] = ((int64_t)zz[b] * ny + yy[a]) * nx;
+            for (int b = 0; b < 3; ++b) r[a][b] = ((IDX)zz[b] * ny + yy[a]) * nx;
         xs[0] = x == 0 ? nx - 1 : x - 1;
         xs[1] = x;
         xs[2] = x == nx - 1 ? 0 : x + 1;
     }
-    __device__ __forceinline__ int64_t at(int dx, int dy, int dz) const { return r[dy + 1][dz + 1] + xs[dx + 1]; }
+    __device__ __forceinline__ IDX at(int dx, int dy, int dz) const { return r[dy + 1][dz + 1] + xs[dx + 1]; }
 };
 
 // ---------------------------------------------------------------------------
 // Odd step: one cell per thread, rows of blockDim.x cells per block iteration.
 // ---------------------------------------------------------------------------
-template <class ST, bool MASK, int MODE>
-__global__ void __launch_bounds__(256, 2) aa_odd(AAParams p) {
+template <class ST, bool MASK, int MODE, class IDX>
+__global__ void __launch_bounds__(256, 3) aa_odd(AAParams p) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     using T = typename ST::T;
     T* __restrict__ f = static_cast<T*>(p.f);
-    const int64_t N = p.N;
+    const IDX N = (IDX)p.N;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const int bx = blockDim.x;
     const int segs = (nx + bx - 1) / bx;
-    const int64_t total = (int64_t)segs * ny * nz;
+    const IDX total = (IDX)segs * ny * nz;
+    const float kin = 1.0f + 3.0f * p.u_in + 3.0f * p.u_in * p.u_in;
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
 
-    for (int64_t sg = blockIdx.x; sg < total; sg += gridDim.x) {
-        const int64_t row = sg / segs;
+    for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
+        const IDX row = sg / segs;
         const int x = (int)(sg - row * segs) * bx + threadIdx.x;
         if (x >= nx) continue;
         const int y = (int)(row % ny);
         const int z = (int)(row / ny);
-        const int64_t id = row * nx + x;
+        const IDX id = row * nx + x;
         const uint32_t fl = MASK ? p.flags[id] : 0u;
         if (MASK && (fl & F_SOLID)) {
             if (MACRO) { p.rho[id] = 1.f; p.ux[id] = 0.f; p.uy[id] = 0.f; p.uz[id] = 0.f; }
             continue;
         }
-        Nbr nb;
+        Nbr<IDX> nb;
         nb.init(x, y, z, nx, ny, nz);
-        const bool special = MASK && (fl & F_SPECIAL);
-        const uint32_t lk = special ? p.links[id] : 0u;
+        uint32_t lk = 0u;
+        if (MASK && (fl & F_SPECIAL)) lk = p.links[id];
         float c[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            // incoming q travels the link x -> x + c_opp(q)
-            if (special && ((lk >> opp(q)) & 1u)) c[q] = ST::ld(f + q * N + id, q, p.rho0);
-            else c[q] = ST::ld(f + opp(q) * N + nb.at(-cx(q), -cy(q), -cz(q)), q, p.rho0);
+            // incoming q travels the link x -> x + c_opp(q); if that link does not
+            // stream, the value was left in the cell's own slot q
+            const bool nn = (lk >> opp(q)) & 1u;
+            const IDX src = nn ? ((IDX)q * N + id) : ((IDX)opp(q) * N + nb.at(-cx(q), -cy(q), -cz(q)));
+            c[q] = ST::ld(f + src, q, p.rho0);
         }
         const Cell m = moments(c, p.fx, p.fy, p.fz);
+        const float om = (p.hybrid && !(fl & F_BAND)) ? p.omega_s : p.omega;
         float o[19];
-        const bool bgk = !p.hybrid || (fl & F_BAND);
-        collide(c, o, m, bgk, p.omega, p.omega_h, p.omega_s);
+#pragma unroll
+        for (int q = 0; q < 19; ++q) o[q] = c[q];
+        collide(o, m, om);
+        const bool at_in = p.duct && x == 0, at_out = p.duct && x == nx - 1;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            if (special && ((lk >> q) & 1u)) {
-                float v = o[q];                                   // bounce-back
-                if (p.duct) {
-                    const int xt = x + cx(q);
-                    if (xt < 0) v = feq_ref(opp(q), m.r, p.u_in, 0.f, 0.f);   // inlet
-                    else if (xt >= nx) v = o[opp(q)];                          // outlet
-                }
-                ST::st(f + opp(q) * N + id, q, p.rho0, v);
-            } else {
-                ST::st(f + q * N + nb.at(cx(q), cy(q), cz(q)), q, p.rho0, o[q]);
-            }
+            const bool nn = (lk >> q) & 1u;
+            float v = o[q];
+            if (cx(q) < 0) v = (nn && at_in) ? inlet_value(q, m.r, kin) : v;
+            if (cx(q) > 0) v = (nn && at_out) ? o[opp(q)] : v;
+            const IDX dst = nn ? ((IDX)opp(q) * N + id) : ((IDX)q * N + nb.at(cx(q), cy(q), cz(q)));
+            ST::st(f + dst, q, p.rho0, v);
         }
         if (MACRO) { p.rho[id] = m.r; p.ux[id] = m.ux; p.uy[id] = m.uy; p.uz[id] = m.uz; }
         if (STATS) {
@@ -284,7 +299,7 @@ __global__ void aa_materialize(AAParams p, int parity, float* __restrict__ out) 
         }
         const int x = (int)(id % p.nx);
         const int64_t row = id / p.nx;
-        Nbr nb;
+        Nbr<int64_t> nb;
         nb.init(x, (int)(row % p.ny), (int)(row / p.ny), p.nx, p.ny, p.nz);
         const uint32_t lk = (fl & F_SPECIAL) ? p.links[id] : 0u;
 #pragma unroll
@@ -297,31 +312,38 @@ __global__ void aa_materialize(AAParams p, int parity, float* __restrict__ out) 
     }
 }
 
-template <class ST, int MODE>
+template <class ST, int MODE, class IDX>
 void launch_mode(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
     const bool mask = p.flags != nullptr;
     // two consecutive cells per thread: 8-byte (F32) or 4-byte (F16/BF16) accesses
     constexpr int V = 2;
     if (parity == 0) {
         if (p.N % V == 0) {
-            if (mask) aa_even<ST, true, V, MODE><<<cfg.blocks, cfg.threads, 0, s>>>(p);
-            else aa_even<ST, false, V, MODE><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+            if (mask) aa_even<ST, true, V, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+            else aa_even<ST, false, V, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
         } else {
-            if (mask) aa_even<ST, true, 1, MODE><<<cfg.blocks, cfg.threads, 0, s>>>(p);
-            else aa_even<ST, false, 1, MODE><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+            if (mask) aa_even<ST, true, 1, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+            else aa_even<ST, false, 1, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
         }
     } else {
-        if (mask) aa_odd<ST, true, MODE><<<cfg.blocks, cfg.threads, 0, s>>>(p);
-        else aa_odd<ST, false, MODE><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+        if (mask) aa_odd<ST, true, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+        else aa_odd<ST, false, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
     }
+}
+
+template <class ST, class IDX>
+void launch_idx(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
+    const int mode = p.stats ? 2 : (p.macro ? 1 : 0);
+    if (mode == 0) launch_mode<ST, 0, IDX>(p, parity, cfg, s);
+    else if (mode == 1) launch_mode<ST, 1, IDX>(p, parity, cfg, s);
+    else launch_mode<ST, 2, IDX>(p, parity, cfg, s);
 }
 
 template <class ST>
 cudaError_t launch_typed(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
-    const int mode = p.stats ? 2 : (p.macro ? 1 : 0);
-    if (mode == 0) launch_mode<ST, 0>(p, parity, cfg, s);
-    else if (mode == 1) launch_mode<ST, 1>(p, parity, cfg, s);
-    else launch_mode<ST, 2>(p, parity, cfg, s);
+    // 32-bit element offsets while every slot index 19*N fits in them
+    if ((uint64_t)p.N * 19u < (1ull << 32)) launch_idx<ST, uint32_t>(p, parity, cfg, s);
+    else launch_idx<ST, int64_t>(p, parity, cfg, s);
     return cudaGetLastError();
 }
 

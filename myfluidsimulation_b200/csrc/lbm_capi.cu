@@ -17,7 +17,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/lbm_capi.h"
+#include "lbm_capi.h"
 #include "lbm_internal.h"
 
 namespace lbm {
@@ -57,6 +57,7 @@ struct lbm_solver {
     bool any_solid = false;
     bool any_band = false;
     bool stats_on = false;
+    bool macro_out = true;      // write rho,u on the last substep of each lbm_step
     int last_stat_blocks = 0;
     int parity = 0;             // AA: 0 natural layout, 1 swapped; reference bounce: 0 A current, 1 B
     int64_t steps = 0;
@@ -152,14 +153,15 @@ static int enqueue_steps(lbm_solver* s, int n) {
     for (int i = 0; i < n; ++i) {
         const bool last = (i == n - 1);
         const bool st = last && s->stats_on;
+        const bool mac = last && (s->macro_out || st);
         if (is_ref_push(s)) {
-            lbm::AAParams p = aa_params(s, last, st);
+            lbm::AAParams p = aa_params(s, mac, st);
             CK(lbm::launch_ref_push(p, static_cast<const float*>(cur_pop(s)), static_cast<float*>(other_pop(s)),
                                     s->cfg_odd, s->stream));
             s->parity ^= 1;
             if (st) s->last_stat_blocks = s->cfg_odd.blocks;
         } else if (is_aa(s)) {
-            lbm::AAParams p = aa_params(s, last, st);
+            lbm::AAParams p = aa_params(s, mac, st);
             const lbm::LaunchCfg cfg = s->parity == 0 ? s->cfg_even : s->cfg_odd;
             CK(lbm::launch_aa_step(p, s->storage, s->parity, cfg, s->stream));
             s->parity ^= 1;
@@ -231,7 +233,7 @@ int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out)
     }
     const int sms = lbm::num_sms();
     s->cfg_even = {sms * 8, 256};
-    s->cfg_odd = {sms * 8, 256};
+    s->cfg_odd = {sms * 12, 256};
     // HOME: enough z-chunks to fill the chip a few times
     {
         const int tiles = ((dom->nx + 31) / 32) * ((dom->ny + 7) / 8);
@@ -507,6 +509,13 @@ int lbm_step_count(lbm_solver* s, int64_t* steps) {
 int lbm_enable_stats(lbm_solver* s, int enable) {
     if (!s) { set_error("lbm_enable_stats: null solver"); return LBM_ERR_INVALID; }
     s->stats_on = enable != 0;
+    return LBM_OK;
+}
+
+int lbm_set_macro_output(lbm_solver* s, int enable) {
+    if (!s) { set_error("lbm_set_macro_output: null solver"); return LBM_ERR_INVALID; }
+    s->macro_out = enable != 0;
+    drop_graph(s);
     return LBM_OK;
 }
 

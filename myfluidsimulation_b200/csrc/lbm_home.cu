@@ -4,18 +4,19 @@
 // gathers the 19 incoming populations and stores their moments.
 //
 // The reference rebuilds f_q 19 times per cell from global loads of the
-// neighbour's 10 moments (190 loads and ~1.1 kFLOP per cell).  Here each
-// block owns a 32 x 8 tile of an (x,y) plane and marches along z over a chunk
-// of planes:
-//   * the moments of plane z+1 (tile + 1-cell halo) are prefetched into
-//     registers one iteration ahead, so their loads overlap the gather of z;
-//   * every cell's 19 post-collision populations are built ONCE, from the
-//     identity  f*_q = w_q [rho + 3 c_q.(rho u) + 4.5 Q_q : (rho u u + (1-w) S)]
-//     with Q_q = c_q c_q - I/3, which is src/lbm/lbm3d_home.cu:57-80
-//     rearranged (4.5(c.u)^2 - 1.5u^2 = 4.5 Q:uu), and kept in shared memory,
-//     grouped by c_z: the 5 down-going ones of plane z+1, the 9 in-plane ones
-//     of planes z and z+1, the 5 up-going ones of planes z-1, z and z+1;
-//   * the gather is then 19 shared-memory loads per cell.
+// neighbour's 10 moments (190 loads and ~1.1 kFLOP per cell).  Here a block
+// owns a 32 x 8 tile of an (x,y) plane and marches along z over a chunk of
+// planes, with one thread per tile cell (8 warps) and 3 warps for the halo:
+//   * each thread keeps the rebuild coefficients of its cell for planes z-1,
+//     z and z+1 in registers (10 each, from the identity
+//         f*_q = w_q [rho + 3 c_q.(rho u) + 4.5 Q_q : (rho u u + (1-w) S)],
+//     Q_q = c_q c_q - I/3, which is src/lbm/lbm3d_home.cu:57-80 rearranged:
+//     4.5 (c.u)^2 - 1.5 u^2 = 4.5 Q:uu), and the moments of plane z+2 in flight;
+//   * per plane it writes to shared memory exactly the populations that cross
+//     into a tile cell: the 5 up-going ones of plane z-1, the 9 in-plane ones
+//     of plane z and the 5 down-going ones of plane z+1 (halo cells only the
+//     5, or 1, that point into the tile), each built once, in opposite-pair form;
+//   * the gather is 19 shared-memory loads and pair sums.
 // DRAM traffic is the 10 moments read once and written once (80 B per cell in
 // FP32) plus the halo re-reads that L2 does not absorb.
 #include "lbm_common.cuh"
@@ -28,23 +29,25 @@ constexpr int TX = 32;
 constexpr int TY = 8;
 constexpr int HX = TX + 2;
 constexpr int HY = TY + 2;
-constexpr int HC = HX * HY;       // 340 halo-tile cells
-constexpr int NT = TX * TY;       // 256 threads
-constexpr int PER = (HC + NT - 1) / NT;   // halo cells per thread (2)
+constexpr int HC = HX * HY;           // 340 halo-tile positions
+constexpr int NWARP = TY + 3;         // 8 tile rows, 2 halo rows, 1 halo-column/corner warp
+constexpr int NT = NWARP * 32;        // 352 threads
 
-// c_z groups in q order
-__host__ __device__ constexpr int grp(int q) { return cz(q) > 0 ? 2 : (cz(q) < 0 ? 0 : 1); }
-__host__ __device__ constexpr int gidx(int q) {
-    // position of q inside its group
-    int k = 0;
-    for (int i = 0; i < q; ++i) k += (grp(i) == grp(q));
-    return k;
+// smem: [UP 5][MID 9][DN 5] x HC floats
+constexpr int UP_OFF = 0, MID_OFF = 5 * HC, DN_OFF = 14 * HC;
+constexpr int SMEM_FLOATS = 19 * HC;
+
+// position of q's plane within the c_z groups (q order inside each group):
+//   c_z = +1 (UP):  5, 11, 12, 15, 16
+//   c_z =  0 (MID): 0, 1, 2, 3, 4, 7, 8, 9, 10
+//   c_z = -1 (DN):  6, 13, 14, 17, 18
+__host__ __device__ constexpr int slot(int q) {
+    constexpr int t[19] = {MID_OFF + 0 * HC, MID_OFF + 1 * HC, MID_OFF + 2 * HC, MID_OFF + 3 * HC, MID_OFF + 4 * HC,
+                           UP_OFF + 0 * HC,  DN_OFF + 0 * HC,  MID_OFF + 5 * HC, MID_OFF + 6 * HC, MID_OFF + 7 * HC,
+                           MID_OFF + 8 * HC, UP_OFF + 1 * HC,  UP_OFF + 2 * HC,  DN_OFF + 1 * HC,  DN_OFF + 2 * HC,
+                           UP_OFF + 3 * HC,  UP_OFF + 4 * HC,  DN_OFF + 3 * HC,  DN_OFF + 4 * HC};
+    return t[q];
 }
-// shared layout offsets (floats)
-constexpr int DN_OFF = 0;                   // [5][HC]   plane z+1
-constexpr int MID_OFF = 5 * HC;             // [2][9][HC] planes by parity
-constexpr int UP_OFF = MID_OFF + 18 * HC;   // [3][5][HC] planes mod 3
-constexpr int SMEM_FLOATS = UP_OFF + 15 * HC;
 
 // Moment storage: F32 as is; F16/BF16 keep rho - rho0, u and S.
 template <class T> struct MomStore;
@@ -69,46 +72,138 @@ template <> struct MomStore<__nv_bfloat16> {
     }
 };
 
-// The 10 regularised-rebuild coefficients of one cell.
+// Rebuild coefficients of one cell, pre-scaled by w1 = 1/18 (w0 = 6 w1, w2 = w1/2):
+//   P = w1 (rho - 1.5 tr B),  a_k = 3 w1 rho u_k,  b_kk = 4.5 w1 B_kk,  b_kl = 9 w1 B_kl,
+//   B = rho u u + (1 - w) S.  Then f*_q = P + sum_k c_k a_k + sum_k c_k^2 b_kk
+//   + sum_{k<l} c_k c_l b_kl for the axis directions, half of that for the
+//   diagonals, and 6 P for the rest direction.
 struct Coef {
     float P, ax, ay, az, bxx, byy, bzz, bxy, bxz, byz;
-    __device__ __forceinline__ void from_moments(const float (&m)[10], float omw) {
+    __device__ __forceinline__ void set(const float (&m)[10], float omw) {
         const float r = m[0];
-        ax = r * m[1]; ay = r * m[2]; az = r * m[3];
-        bxx = ax * m[1] + omw * m[4];
-        bxy = ax * m[2] + omw * m[5];
-        bxz = ax * m[3] + omw * m[6];
-        byy = ay * m[2] + omw * m[7];
-        byz = ay * m[3] + omw * m[8];
-        bzz = az * m[3] + omw * m[9];
-        P = r - 1.5f * (bxx + byy + bzz);
+        const float jx = r * m[1], jy = r * m[2], jz = r * m[3];
+        const float Bxx = fmaf(jx, m[1], omw * m[4]);
+        const float Bxy = fmaf(jx, m[2], omw * m[5]);
+        const float Bxz = fmaf(jx, m[3], omw * m[6]);
+        const float Byy = fmaf(jy, m[2], omw * m[7]);
+        const float Byz = fmaf(jy, m[3], omw * m[8]);
+        const float Bzz = fmaf(jz, m[3], omw * m[9]);
+        constexpr float w1 = 1.0f / 18.0f;
+        P = w1 * fmaf(-1.5f, Bxx + Byy + Bzz, r);
+        ax = (3.0f * w1) * jx; ay = (3.0f * w1) * jy; az = (3.0f * w1) * jz;
+        bxx = (4.5f * w1) * Bxx; byy = (4.5f * w1) * Byy; bzz = (4.5f * w1) * Bzz;
+        bxy = (9.0f * w1) * Bxy; bxz = (9.0f * w1) * Bxz; byz = (9.0f * w1) * Byz;
     }
-    // f*_q = w_q [P + 3 c.a + 4.5 sum_a c_a^2 B_aa + 9 sum_{a<b} c_a c_b B_ab]
+    // one population (halo positions and the boundary path)
     template <int q>
     __device__ __forceinline__ float fpost() const {
-        float s = P;
         constexpr int X = cx(q), Y = cy(q), Z = cz(q);
-        if (X) s += (X > 0 ? 3.f : -3.f) * ax;
-        if (Y) s += (Y > 0 ? 3.f : -3.f) * ay;
-        if (Z) s += (Z > 0 ? 3.f : -3.f) * az;
-        if (X) s += 4.5f * bxx;
-        if (Y) s += 4.5f * byy;
-        if (Z) s += 4.5f * bzz;
-        if (X && Y) s += (X * Y > 0 ? 9.f : -9.f) * bxy;
-        if (X && Z) s += (X * Z > 0 ? 9.f : -9.f) * bxz;
-        if (Y && Z) s += (Y * Z > 0 ? 9.f : -9.f) * byz;
-        return wq(q) * s;
+        if constexpr (q == 0) {
+            return 6.0f * P;
+        } else {
+            float s = P;
+            if (X) s += X > 0 ? ax : -ax;
+            if (Y) s += Y > 0 ? ay : -ay;
+            if (Z) s += Z > 0 ? az : -az;
+            if (X) s += bxx;
+            if (Y) s += byy;
+            if (Z) s += bzz;
+            if (X && Y) s += X * Y > 0 ? bxy : -bxy;
+            if (X && Z) s += X * Z > 0 ? bxz : -bxz;
+            if (Y && Z) s += Y * Z > 0 ? byz : -byz;
+            return ((X != 0) + (Y != 0) + (Z != 0)) == 2 ? 0.5f * s : s;
+        }
     }
 };
 
-template <int q>
-struct QI { static constexpr int value = q; };
-
+template <int q> struct QI { static constexpr int value = q; };
 template <int Q0, int Q1, class F>
 __device__ __forceinline__ void static_for(F&& fn) {
     if constexpr (Q0 < Q1) {
         fn(QI<Q0>{});
         static_for<Q0 + 1, Q1>(fn);
+    }
+}
+
+// A tile cell writes its 5 up-going populations of plane z-1 (from `up`), its 9
+// in-plane ones of plane z (`mid`) and its 5 down-going ones of plane z+1 (`dn`),
+// except for the planes where the cell is solid.
+__device__ __forceinline__ void build_tile_cell(float* sm, int pos, const Coef& up, const Coef& mid, const Coef& dn,
+                                                bool s_up, bool s_mid, bool s_dn) {
+    if (!s_up) {
+        const Coef& c = up;
+        const float bz = c.P + c.bzz;
+        sm[slot(5) + pos] = bz + c.az;
+        const float bxz = bz + c.bxx, byz = bz + c.byy;
+        sm[slot(11) + pos] = 0.5f * (bxz + c.bxz + c.ax + c.az);    // (+1,0,+1)
+        sm[slot(12) + pos] = 0.5f * (bxz - c.bxz - c.ax + c.az);    // (-1,0,+1)
+        sm[slot(15) + pos] = 0.5f * (byz + c.byz + c.ay + c.az);    // (0,+1,+1)
+        sm[slot(16) + pos] = 0.5f * (byz - c.byz - c.ay + c.az);    // (0,-1,+1)
+    }
+    if (!s_mid) {
+        const Coef& c = mid;
+        sm[slot(0) + pos] = 6.0f * c.P;
+        const float bx = c.P + c.bxx, by = c.P + c.byy;
+        sm[slot(1) + pos] = bx + c.ax;
+        sm[slot(2) + pos] = bx - c.ax;
+        sm[slot(3) + pos] = by + c.ay;
+        sm[slot(4) + pos] = by - c.ay;
+        const float bxy = bx + c.byy;
+        const float bp = bxy + c.bxy, bm = bxy - c.bxy;
+        const float sp = c.ax + c.ay, sn = c.ax - c.ay;
+        sm[slot(7) + pos] = 0.5f * (bp + sp);     // (+1,+1,0)
+        sm[slot(10) + pos] = 0.5f * (bp - sp);    // (-1,-1,0)
+        sm[slot(9) + pos] = 0.5f * (bm + sn);     // (+1,-1,0)
+        sm[slot(8) + pos] = 0.5f * (bm - sn);     // (-1,+1,0)
+    }
+    if (!s_dn) {
+        const Coef& c = dn;
+        const float bz = c.P + c.bzz;
+        sm[slot(6) + pos] = bz - c.az;
+        const float bxz = bz + c.bxx, byz = bz + c.byy;
+        sm[slot(13) + pos] = 0.5f * (bxz - c.bxz + c.ax - c.az);    // (+1,0,-1)
+        sm[slot(14) + pos] = 0.5f * (bxz + c.bxz - c.ax - c.az);    // (-1,0,-1)
+        sm[slot(17) + pos] = 0.5f * (byz - c.byz + c.ay - c.az);    // (0,+1,-1)
+        sm[slot(18) + pos] = 0.5f * (byz + c.byz - c.ay - c.az);    // (0,-1,-1)
+    }
+}
+
+// A halo position contributes only the directions that point into the tile:
+// one in-plane axis + two in-plane diagonals + one up + one down (edges), or one
+// in-plane diagonal (corners).  dir: 0 = x-1 column (+x), 1 = x+TX column (-x),
+// 2 = y-1 row (+y), 3 = y+TY row (-y), 4..7 = corners feeding 7, 8, 9, 10.
+__device__ __forceinline__ void build_halo(float* sm, int pos, int dir, const Coef& up, const Coef& mid,
+                                           const Coef& dn, bool s_up, bool s_mid, bool s_dn) {
+    switch (dir) {
+        case 0:
+            if (!s_mid) { sm[slot(1) + pos] = mid.fpost<1>(); sm[slot(7) + pos] = mid.fpost<7>();
+                          sm[slot(9) + pos] = mid.fpost<9>(); }
+            if (!s_up) sm[slot(11) + pos] = up.fpost<11>();
+            if (!s_dn) sm[slot(13) + pos] = dn.fpost<13>();
+            break;
+        case 1:
+            if (!s_mid) { sm[slot(2) + pos] = mid.fpost<2>(); sm[slot(8) + pos] = mid.fpost<8>();
+                          sm[slot(10) + pos] = mid.fpost<10>(); }
+            if (!s_up) sm[slot(12) + pos] = up.fpost<12>();
+            if (!s_dn) sm[slot(14) + pos] = dn.fpost<14>();
+            break;
+        case 2:
+            if (!s_mid) { sm[slot(3) + pos] = mid.fpost<3>(); sm[slot(7) + pos] = mid.fpost<7>();
+                          sm[slot(8) + pos] = mid.fpost<8>(); }
+            if (!s_up) sm[slot(15) + pos] = up.fpost<15>();
+            if (!s_dn) sm[slot(17) + pos] = dn.fpost<17>();
+            break;
+        case 3:
+            if (!s_mid) { sm[slot(4) + pos] = mid.fpost<4>(); sm[slot(9) + pos] = mid.fpost<9>();
+                          sm[slot(10) + pos] = mid.fpost<10>(); }
+            if (!s_up) sm[slot(16) + pos] = up.fpost<16>();
+            if (!s_dn) sm[slot(18) + pos] = dn.fpost<18>();
+            break;
+        case 4: if (!s_mid) sm[slot(7) + pos] = mid.fpost<7>(); break;
+        case 5: if (!s_mid) sm[slot(8) + pos] = mid.fpost<8>(); break;
+        case 6: if (!s_mid) sm[slot(9) + pos] = mid.fpost<9>(); break;
+        case 7: if (!s_mid) sm[slot(10) + pos] = mid.fpost<10>(); break;
+        default: break;
     }
 }
 
@@ -125,168 +220,156 @@ __global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
     const int tiles_x = (nx + TX - 1) / TX;
     const int tiles_y = (ny + TY - 1) / TY;
     int b = blockIdx.x;
-    const int tx0 = (b % tiles_x) * TX; b /= tiles_x;
-    const int ty0 = (b % tiles_y) * TY; b /= tiles_y;
+    const int x0 = (b % tiles_x) * TX; b /= tiles_x;
+    const int y0 = (b % tiles_y) * TY; b /= tiles_y;
     const int z0 = b * p.zchunk;
     const int z1 = min(nz, z0 + p.zchunk);
-    const int tid = threadIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    // halo cells staged by this thread
-    int64_t hoff[PER];     // plane-relative offset, -1 if outside / not mine
-#pragma unroll
-    for (int k = 0; k < PER; ++k) {
-        const int i = tid + k * NT;
-        hoff[k] = -1;
-        if (i < HC) {
-            int gx = tx0 - 1 + (i % HX);
-            int gy = ty0 - 1 + (i / HX);
-            gy = ((gy % ny) + ny) % ny;
-            bool ok = true;
-            if (p.duct) ok = (gx >= 0 && gx < nx);
-            else gx = ((gx % nx) + nx) % nx;
-            if (ok) hoff[k] = (int64_t)gy * nx + gx;
-        }
-    }
+    // this thread's position in the (TX+2) x (TY+2) halo tile, and its role
+    int hx, hy, dir;   // dir: -1 tile cell, 0..7 halo (see build_halo), -2 idle
+    if (warp < TY) { hx = lane + 1; hy = warp + 1; dir = -1; }
+    else if (warp == TY) { hx = lane + 1; hy = 0; dir = 2; }
+    else if (warp == TY + 1) { hx = lane + 1; hy = TY + 1; dir = 3; }
+    else if (lane < TY) { hx = 0; hy = lane + 1; dir = 0; }
+    else if (lane < 2 * TY) { hx = TX + 1; hy = lane - TY + 1; dir = 1; }
+    else if (lane < 2 * TY + 4) {
+        const int k = lane - 2 * TY;
+        hx = (k & 1) ? TX + 1 : 0; hy = (k & 2) ? TY + 1 : 0; dir = 4 + k;
+    } else { hx = 0; hy = 0; dir = -2; }
+    const int pos = hy * HX + hx;
+    // the cell it stands for (periodic in y, periodic or absent in x)
+    const int lx = x0 - 1 + hx, ly = y0 - 1 + hy;
+    int gx = lx;
+    const int gy = ((ly % ny) + ny) % ny;
+    bool exists = dir != -2;
+    if (p.duct) exists = exists && lx >= 0 && lx < nx;
+    else gx = ((lx % nx) + nx) % nx;
+    const bool owner = dir == -1 && lx < nx && ly < ny;   // gathers and stores a cell
     const int64_t plane = (int64_t)nx * ny;
-    float reg[PER][10];
-    auto load_plane = [&](int z) {
+    const int64_t coff = (int64_t)gy * nx + gx;
+
+    const uint8_t* __restrict__ flags = p.flags;
+    float mreg[10];
+#pragma unroll
+    for (int c = 0; c < 10; ++c) mreg[c] = 0.f;
+    uint32_t freg = 0;
+    auto load = [&](int z) {
+        if (!exists) return;
         const int zz = ((z % nz) + nz) % nz;
+        const int64_t id = (int64_t)zz * plane + coff;
+        const T* ptr = m + id;
 #pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            if (hoff[k] < 0) continue;
-            const int64_t id = (int64_t)zz * plane + hoff[k];
-#pragma unroll
-            for (int c = 0; c < 10; ++c) reg[k][c] = MomStore<T>::ld(m + c * N + id, c, r0);
+        for (int c = 0; c < 10; ++c) {
+            mreg[c] = MomStore<T>::ld(ptr, c, r0);
+            ptr += N;
         }
+        freg = flags ? flags[id] : 0u;
     };
-    // builds the populations of the staged plane z into shared memory;
-    // which = 1: only the up-going group, 2: up-going + in-plane, 3: all
-    auto build_plane = [&](int z, int which) {
-        float* up = sm + UP_OFF + (((z % 3) + 3) % 3) * 5 * HC;
-        float* mid = sm + MID_OFF + (z & 1) * 9 * HC;
-        float* dn = sm + DN_OFF;
-#pragma unroll
-        for (int k = 0; k < PER; ++k) {
-            const int i = tid + k * NT;
-            if (hoff[k] < 0) continue;
-            Coef cf;
-            cf.from_moments(reg[k], omw);
-            static_for<0, 19>([&](auto qi) {
-                constexpr int q = decltype(qi)::value;
-                constexpr int g = grp(q), j = gidx(q);
-                if (g == 2) up[j * HC + i] = cf.template fpost<q>();
-                else if (g == 1) { if (which >= 2) mid[j * HC + i] = cf.template fpost<q>(); }
-                else { if (which >= 3) dn[j * HC + i] = cf.template fpost<q>(); }
-            });
-        }
-    };
+    // rebuild coefficients and flag bytes of this position for planes z-1, z, z+1
+    Coef C0, C1, C2;
+    uint32_t F0, F1, F2;
+    load(z0 - 1);
+    C0.set(mreg, omw); F0 = freg;
+    load(z0);
+    C1.set(mreg, omw); F1 = freg;
+    load(z0 + 1);
+    C2.set(mreg, omw); F2 = freg;
+    if (z0 + 2 <= z1) load(z0 + 2);
 
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
 
-    const int lx = tid % TX, ly = tid / TX;
-    const int gx = tx0 + lx, gy = ty0 + ly;
-    const bool inside = gx < nx && gy < ny;
-    const int hc = (ly + 1) * HX + (lx + 1);
-
-    load_plane(z0 - 1);
-    build_plane(z0 - 1, 1);
-    load_plane(z0);
-    build_plane(z0, 2);
-    load_plane(z0 + 1);
     for (int z = z0; z < z1; ++z) {
-        build_plane(z + 1, 3);
-        if (z + 1 < z1) load_plane(z + 2);
+        // 1. populations into the tile: a solid cell contributes nothing (its
+        //    slots are the ones its fluid neighbours fill in step 2)
+        if (exists) {
+            if (dir == -1) build_tile_cell(sm, pos, C0, C1, C2, F0 & F_SOLID, F1 & F_SOLID, F2 & F_SOLID);
+            else build_halo(sm, pos, dir, C0, C1, C2, F0 & F_SOLID, F1 & F_SOLID, F2 & F_SOLID);
+        }
+        // 2. a link that does not stream: the cell writes the replacement into the
+        //    slot of the source it would have gathered from (read by nobody else)
+        if (owner && (F1 & F_SPECIAL)) {
+            const int64_t id = (int64_t)z * plane + coff;
+            const uint32_t lk = p.links[id];
+            float rho_own = 0.f;
+            if (p.duct && (gx == 0)) rho_own = MomStore<T>::ld(m + id, 0, r0);
+            static_for<1, 19>([&](auto qi) {
+                constexpr int q = decltype(qi)::value;
+                if ((lk >> opp(q)) & 1u) {
+                    const int xs = gx - cx(q);
+                    float v;
+                    if (p.duct && xs < 0) {
+                        v = feq_ref(q, rho_own, p.u_in, 0.f, 0.f);                      // inlet
+                    } else if (p.duct && xs >= nx) {
+                        v = C1.template fpost<q>();                                        // outlet
+                    } else {
+                        // own post-collision population of direction bq comes back as q
+                        // (home.cu:219-225); bq = opp(q), or the reference's table
+                        constexpr int bt = opp(q), br = opp_tab(q);
+                        v = p.ref_bounce ? C1.template fpost<br>() : C1.template fpost<bt>();
+                        if (STATS) {
+                            const int bq = p.ref_bounce ? br : bt;
+                            const int ys = ((gy - cy(q)) % ny + ny) % ny;
+                            const int zs = ((z - cz(q)) % nz + nz) % nz;
+                            const int xw = ((xs % nx) + nx) % nx;
+                            if (flags[(int64_t)zs * plane + (int64_t)ys * nx + xw] & F_OBST) {
+                                acc[2] += (double)(cx(bq) - cx(q)) * (double)v;
+                                acc[3] += (double)(cy(bq) - cy(q)) * (double)v;
+                                acc[4] += (double)(cz(bq) - cz(q)) * (double)v;
+                            }
+                        }
+                    }
+                    sm[slot(q) + pos - cx(q) - HX * cy(q)] = v;
+                }
+            });
+        }
         __syncthreads();
-        if (inside) {
-            const int64_t id = (int64_t)z * plane + (int64_t)gy * nx + gx;
-            const uint32_t fl = p.flags ? p.flags[id] : 0u;
-            if (fl & F_SOLID) {
-                MomStore<T>::st(mn + id, 0, r0, 1.f);
+        // 3. gather and moments
+        if (owner) {
+            const int64_t id = (int64_t)z * plane + coff;
+            T* op = mn + id;
+            if (F1 & F_SOLID) {
+                MomStore<T>::st(op, 0, r0, 1.f);
 #pragma unroll
-                for (int c = 1; c < 10; ++c) MomStore<T>::st(mn + c * N + id, c, r0, 0.f);
+                for (int c = 1; c < 10; ++c) MomStore<T>::st(op + c * N, c, r0, 0.f);
             } else {
-                const float* up = sm + UP_OFF + (((z - 1) % 3 + 3) % 3) * 5 * HC;
-                const float* mid = sm + MID_OFF + (z & 1) * 9 * HC;
-                const float* dn = sm + DN_OFF;
                 float fq[19];
                 static_for<0, 19>([&](auto qi) {
                     constexpr int q = decltype(qi)::value;
-                    constexpr int g = grp(q), j = gidx(q);
-                    const int src = hc - cx(q) - HX * cy(q);
-                    fq[q] = (g == 2 ? up : (g == 1 ? mid : dn))[j * HC + src];
+                    fq[q] = sm[slot(q) + pos - cx(q) - HX * cy(q)];
                 });
-                if (fl & F_SPECIAL) {
-                    // links that do not stream: rebuild from the cell's own moments
-                    const uint32_t lk = p.links[id];
-                    float own[10];
-#pragma unroll
-                    for (int c = 0; c < 10; ++c) own[c] = MomStore<T>::ld(m + c * N + id, c, r0);
-                    Coef oc;
-                    oc.from_moments(own, omw);
-                    float of[19];
-                    static_for<0, 19>([&](auto qi) {
-                        constexpr int q = decltype(qi)::value;
-                        of[q] = oc.template fpost<q>();
-                    });
-                    static_for<1, 19>([&](auto qi) {
-                        constexpr int q = decltype(qi)::value;
-                        if ((lk >> opp(q)) & 1u) {
-                            const int xs = gx - cx(q);
-                            if (p.duct && xs < 0) {
-                                fq[q] = feq_ref(q, own[0], p.u_in, 0.f, 0.f);          // inlet
-                            } else if (p.duct && xs >= nx) {
-                                fq[q] = of[q];                                           // outlet
-                            } else {
-                                // own post-collision population of direction b comes back as q
-                                // (home.cu:219-225); b = opp(q), or the reference's table
-                                constexpr int b_true = opp(q), b_tab = opp_tab(q);
-                                const int b = p.ref_bounce ? b_tab : b_true;
-                                fq[q] = p.ref_bounce ? of[b_tab] : of[b_true];
-                                if (STATS && (fl & F_TOUCH)) {
-                                    const int ys = ((gy - cy(q)) % ny + ny) % ny;
-                                    const int zs = ((z - cz(q)) % nz + nz) % nz;
-                                    const int xw = ((xs % nx) + nx) % nx;
-                                    if (p.flags[(int64_t)zs * plane + (int64_t)ys * nx + xw] & F_OBST) {
-                                        acc[2] += (double)(cx(b) - cx(q)) * (double)fq[q];
-                                        acc[3] += (double)(cy(b) - cy(q)) * (double)fq[q];
-                                        acc[4] += (double)(cz(b) - cz(q)) * (double)fq[q];
-                                    }
-                                }
-                            }
-                        }
-                    });
-                }
-                // moments of the gathered populations (home.cu:238-273)
-                float r = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-                float Mxx = 0.f, Mxy = 0.f, Mxz = 0.f, Myy = 0.f, Myz = 0.f, Mzz = 0.f;
-                static_for<0, 19>([&](auto qi) {
-                    constexpr int q = decltype(qi)::value;
-                    constexpr int X = cx(q), Y = cy(q), Z = cz(q);
-                    const float v = fq[q];
-                    r += v;
-                    if (X) jx += X > 0 ? v : -v;
-                    if (Y) jy += Y > 0 ? v : -v;
-                    if (Z) jz += Z > 0 ? v : -v;
-                    if (X) Mxx += v;
-                    if (Y) Myy += v;
-                    if (Z) Mzz += v;
-                    if (X && Y) Mxy += X * Y > 0 ? v : -v;
-                    if (X && Z) Mxz += X * Z > 0 ? v : -v;
-                    if (Y && Z) Myz += Y * Z > 0 ? v : -v;
-                });
-                float ux = (r > 0.f) ? (jx / r) : 0.f;
-                float uy = (r > 0.f) ? (jy / r) : 0.f;
-                float uz = (r > 0.f) ? (jz / r) : 0.f;
-                ux += p.fx; uy += p.fy; uz += p.fz;
-                const float cs2 = 1.0f / 3.0f;
+                // moments of the gathered populations (home.cu:238-273), opposite pairs first
+                const float s1 = fq[1] + fq[2], d1 = fq[1] - fq[2];
+                const float s3 = fq[3] + fq[4], d3 = fq[3] - fq[4];
+                const float s5 = fq[5] + fq[6], d5 = fq[5] - fq[6];
+                const float s7 = fq[7] + fq[10], d7 = fq[7] - fq[10];     // (+1,+1,0)
+                const float s9 = fq[9] + fq[8], d9 = fq[9] - fq[8];       // (+1,-1,0)
+                const float s11 = fq[11] + fq[14], d11 = fq[11] - fq[14]; // (+1,0,+1)
+                const float s13 = fq[13] + fq[12], d13 = fq[13] - fq[12]; // (+1,0,-1)
+                const float s15 = fq[15] + fq[18], d15 = fq[15] - fq[18]; // (0,+1,+1)
+                const float s17 = fq[17] + fq[16], d17 = fq[17] - fq[16]; // (0,+1,-1)
+                const float r = fq[0] + ((s1 + s3) + (s5 + s7)) + ((s9 + s11) + (s13 + s15) + s17);
+                const float jx = (d1 + d7) + (d9 + d11) + d13;
+                const float jy = (d3 + d7) - d9 + (d15 + d17);
+                const float jz = (d5 + d11) - d13 + (d15 - d17);
+                const float Mxx = (s1 + s7) + (s9 + s11) + s13;
+                const float Myy = (s3 + s7) + (s9 + s15) + s17;
+                const float Mzz = (s5 + s11) + (s13 + s15) + s17;
+                const float Mxy = s7 - s9, Mxz = s11 - s13, Myz = s15 - s17;
+                const float inv = r > 0.f ? 1.0f / r : 0.f;
+                const float ux = jx * inv + p.fx, uy = jy * inv + p.fy, uz = jz * inv + p.fz;
+                const float r3 = r * (1.0f / 3.0f);
+                const float rx = r * ux, ry = r * uy, rz = r * uz;
                 const float out[10] = {r, ux, uy, uz,
-                                       Mxx - (r * cs2 + r * ux * ux), Mxy - r * ux * uy, Mxz - r * ux * uz,
-                                       Myy - (r * cs2 + r * uy * uy), Myz - r * uy * uz,
-                                       Mzz - (r * cs2 + r * uz * uz)};
+                                       Mxx - fmaf(rx, ux, r3), Mxy - rx * uy, Mxz - rx * uz,
+                                       Myy - fmaf(ry, uy, r3), Myz - ry * uz, Mzz - fmaf(rz, uz, r3)};
 #pragma unroll
-                for (int c = 0; c < 10; ++c) MomStore<T>::st(mn + c * N + id, c, r0, out[c]);
+                for (int c = 0; c < 10; ++c) {
+                    MomStore<T>::st(op, c, r0, out[c]);
+                    op += N;
+                }
                 if (STATS) {
                     acc[0] += (double)r;
                     acc[1] += 0.5 * ((double)ux * ux + (double)uy * uy + (double)uz * uz);
@@ -297,6 +380,12 @@ __global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
             }
         }
         __syncthreads();
+        if (z + 1 < z1) {
+            C0 = C1; F0 = F1;
+            C1 = C2; F1 = F2;
+            C2.set(mreg, omw); F2 = freg;       // plane z+2, loaded one iteration ago
+            if (z + 3 <= z1) load(z + 3);
+        }
     }
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }

@@ -15,7 +15,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/lbm_capi.h"
+#include "lbm_capi.h"
 
 namespace lbm {
 void set_error(const std::string& msg);

@@ -128,6 +128,9 @@ class Solver:
     def enable_stats(self, on=True):
         check(lib().lbm_enable_stats(self._h, 1 if on else 0))
 
+    def set_macro_output(self, on=True):
+        check(lib().lbm_set_macro_output(self._h, 1 if on else 0))
+
     # -- stepping ----------------------------------------------------------------
     def step(self, n: int = 1):
         """Queue n steps (asynchronous)."""

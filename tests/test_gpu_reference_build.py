@@ -106,7 +106,7 @@ def test_masked_home_matches_reference_build(ref, oracle):
     e_ref = rl2(np.stack([ru, rv, rw]), mo[1:4])          # the reference build against the oracle
     e_mine = rl2(np.stack([mu, mv, mw]), mo[1:4])
     assert e_ref < 3e-4 and e_mine < 3e-4                  # u ~ 5e-4 here: FP32 noise ~1e-4 relative
-    assert rl2(rr, mo[0]) < 1e-6 and rl2(mr, mo[0]) < 1e-6
+    assert rl2(rr, mo[0]) < 3e-6 and rl2(mr, mo[0]) < 3e-6
     assert rl2(np.stack([mu, mv, mw]), np.stack([ru, rv, rw])) < 2 * max(e_ref, e_mine) + 1e-5
 
 

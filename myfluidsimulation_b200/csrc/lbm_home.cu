@@ -7,15 +7,17 @@
 // neighbour's 10 moments (190 loads and ~1.1 kFLOP per cell).  Here a block
 // owns a 32 x 8 tile of an (x,y) plane and marches along z over a chunk of
 // planes, with one thread per tile cell (8 warps) and 3 warps for the halo:
-//   * each thread keeps the rebuild coefficients of its cell for planes z-1,
-//     z and z+1 in registers (10 each, from the identity
+//   * when the moments of a plane arrive (requested one plane ahead), every
+//     position rebuilds its post-collision populations ONCE, from the identity
 //         f*_q = w_q [rho + 3 c_q.(rho u) + 4.5 Q_q : (rho u u + (1-w) S)],
-//     Q_q = c_q c_q - I/3, which is src/lbm/lbm3d_home.cu:57-80 rearranged:
-//     4.5 (c.u)^2 - 1.5 u^2 = 4.5 Q:uu), and the moments of plane z+2 in flight;
-//   * per plane it writes to shared memory exactly the populations that cross
-//     into a tile cell: the 5 up-going ones of plane z-1, the 9 in-plane ones
-//     of plane z and the 5 down-going ones of plane z+1 (halo cells only the
-//     5, or 1, that point into the tile), each built once, in opposite-pair form;
+//     Q_q = c_q c_q - I/3 (src/lbm/lbm3d_home.cu:57-80 rearranged:
+//     4.5 (c.u)^2 - 1.5 u^2 = 4.5 Q:uu), in opposite-pair form, into a shared
+//     ring grouped by c_z: the up-going group lives 3 planes, the in-plane group
+//     2 and the down-going group 1 (38 floats per position; halo positions write
+//     only the 5, or 1, populations that point into the tile);
+//   * a link that does not stream (solid neighbour, duct inlet/outlet) is
+//     handled by the gathering cell, which writes the replacement into the slot
+//     of the source it would have gathered from (each slot has one reader);
 //   * the gather is 19 shared-memory loads and pair sums.
 // DRAM traffic is the 10 moments read once and written once (80 B per cell in
 // FP32) plus the halo re-reads that L2 does not absorb.
@@ -33,21 +35,32 @@ constexpr int HC = HX * HY;           // 340 halo-tile positions
 constexpr int NWARP = TY + 3;         // 8 tile rows, 2 halo rows, 1 halo-column/corner warp
 constexpr int NT = NWARP * 32;        // 352 threads
 
-// smem: [UP 5][MID 9][DN 5] x HC floats
-constexpr int UP_OFF = 0, MID_OFF = 5 * HC, DN_OFF = 14 * HC;
-constexpr int SMEM_FLOATS = 19 * HC;
+// shared ring, grouped by c_z: UP[3][5][HC], MID[2][9][HC], DN[5][HC]
+constexpr int UP_SZ = 5 * HC, MID_SZ = 9 * HC, DN_SZ = 5 * HC;
+constexpr int MID_OFF = 3 * UP_SZ, DN_OFF = MID_OFF + 2 * MID_SZ;
+constexpr int SMEM_FLOATS = DN_OFF + DN_SZ;
 
-// position of q's plane within the c_z groups (q order inside each group):
-//   c_z = +1 (UP):  5, 11, 12, 15, 16
-//   c_z =  0 (MID): 0, 1, 2, 3, 4, 7, 8, 9, 10
-//   c_z = -1 (DN):  6, 13, 14, 17, 18
-__host__ __device__ constexpr int slot(int q) {
-    constexpr int t[19] = {MID_OFF + 0 * HC, MID_OFF + 1 * HC, MID_OFF + 2 * HC, MID_OFF + 3 * HC, MID_OFF + 4 * HC,
-                           UP_OFF + 0 * HC,  DN_OFF + 0 * HC,  MID_OFF + 5 * HC, MID_OFF + 6 * HC, MID_OFF + 7 * HC,
-                           MID_OFF + 8 * HC, UP_OFF + 1 * HC,  UP_OFF + 2 * HC,  DN_OFF + 1 * HC,  DN_OFF + 2 * HC,
-                           UP_OFF + 3 * HC,  UP_OFF + 4 * HC,  DN_OFF + 3 * HC,  DN_OFF + 4 * HC};
-    return t[q];
+// offset of q inside its group (UP: 5,11,12,15,16; MID: 0,1,2,3,4,7,8,9,10; DN: 6,13,14,17,18)
+__host__ __device__ constexpr int gofs(int q) {
+    constexpr int t[19] = {0, 1, 2, 3, 4, 0, 0, 5, 6, 7, 8, 1, 2, 1, 2, 3, 4, 3, 4};
+    return t[q] * HC;
 }
+
+// the ring groups that hold the populations leaving plane p
+struct Ring {
+    float* up;
+    float* mid;
+    float* dn;
+    __device__ __forceinline__ Ring(float* sm, int p) {
+        up = sm + (((p % 3) + 3) % 3) * UP_SZ;
+        mid = sm + MID_OFF + (p & 1) * MID_SZ;
+        dn = sm + DN_OFF;
+    }
+    template <int q>
+    __device__ __forceinline__ float& at(int pos) const {
+        return (cz(q) > 0 ? up : (cz(q) == 0 ? mid : dn))[gofs(q) + pos];
+    }
+};
 
 // Moment storage: F32 as is; F16/BF16 keep rho - rho0, u and S.
 template <class T> struct MomStore;
@@ -125,90 +138,73 @@ __device__ __forceinline__ void static_for(F&& fn) {
     }
 }
 
-// A tile cell writes its 5 up-going populations of plane z-1 (from `up`), its 9
-// in-plane ones of plane z (`mid`) and its 5 down-going ones of plane z+1 (`dn`),
-// except for the planes where the cell is solid.
-__device__ __forceinline__ void build_tile_cell(float* sm, int pos, const Coef& up, const Coef& mid, const Coef& dn,
-                                                bool s_up, bool s_mid, bool s_dn) {
-    if (!s_up) {
-        const Coef& c = up;
-        const float bz = c.P + c.bzz;
-        sm[slot(5) + pos] = bz + c.az;
-        const float bxz = bz + c.bxx, byz = bz + c.byy;
-        sm[slot(11) + pos] = 0.5f * (bxz + c.bxz + c.ax + c.az);    // (+1,0,+1)
-        sm[slot(12) + pos] = 0.5f * (bxz - c.bxz - c.ax + c.az);    // (-1,0,+1)
-        sm[slot(15) + pos] = 0.5f * (byz + c.byz + c.ay + c.az);    // (0,+1,+1)
-        sm[slot(16) + pos] = 0.5f * (byz - c.byz - c.ay + c.az);    // (0,-1,+1)
-    }
-    if (!s_mid) {
-        const Coef& c = mid;
-        sm[slot(0) + pos] = 6.0f * c.P;
-        const float bx = c.P + c.bxx, by = c.P + c.byy;
-        sm[slot(1) + pos] = bx + c.ax;
-        sm[slot(2) + pos] = bx - c.ax;
-        sm[slot(3) + pos] = by + c.ay;
-        sm[slot(4) + pos] = by - c.ay;
-        const float bxy = bx + c.byy;
-        const float bp = bxy + c.bxy, bm = bxy - c.bxy;
+// A tile cell writes all 19 populations leaving its plane.
+__device__ __forceinline__ void build_tile_cell(const Ring& R, int pos, const Coef& c) {
+    R.at<0>(pos) = 6.0f * c.P;
+    const float bx = c.P + c.bxx, by = c.P + c.byy, bz = c.P + c.bzz;
+    R.at<1>(pos) = bx + c.ax;
+    R.at<2>(pos) = bx - c.ax;
+    R.at<3>(pos) = by + c.ay;
+    R.at<4>(pos) = by - c.ay;
+    R.at<5>(pos) = bz + c.az;
+    R.at<6>(pos) = bz - c.az;
+    {
+        const float b = bx + c.byy, bp = b + c.bxy, bm = b - c.bxy;
         const float sp = c.ax + c.ay, sn = c.ax - c.ay;
-        sm[slot(7) + pos] = 0.5f * (bp + sp);     // (+1,+1,0)
-        sm[slot(10) + pos] = 0.5f * (bp - sp);    // (-1,-1,0)
-        sm[slot(9) + pos] = 0.5f * (bm + sn);     // (+1,-1,0)
-        sm[slot(8) + pos] = 0.5f * (bm - sn);     // (-1,+1,0)
+        R.at<7>(pos) = 0.5f * (bp + sp);     // (+1,+1,0)
+        R.at<10>(pos) = 0.5f * (bp - sp);    // (-1,-1,0)
+        R.at<9>(pos) = 0.5f * (bm + sn);     // (+1,-1,0)
+        R.at<8>(pos) = 0.5f * (bm - sn);     // (-1,+1,0)
     }
-    if (!s_dn) {
-        const Coef& c = dn;
-        const float bz = c.P + c.bzz;
-        sm[slot(6) + pos] = bz - c.az;
-        const float bxz = bz + c.bxx, byz = bz + c.byy;
-        sm[slot(13) + pos] = 0.5f * (bxz - c.bxz + c.ax - c.az);    // (+1,0,-1)
-        sm[slot(14) + pos] = 0.5f * (bxz + c.bxz - c.ax - c.az);    // (-1,0,-1)
-        sm[slot(17) + pos] = 0.5f * (byz - c.byz + c.ay - c.az);    // (0,+1,-1)
-        sm[slot(18) + pos] = 0.5f * (byz + c.byz - c.ay - c.az);    // (0,-1,-1)
+    {
+        const float b = bx + c.bzz, bp = b + c.bxz, bm = b - c.bxz;
+        const float sp = c.ax + c.az, sn = c.ax - c.az;
+        R.at<11>(pos) = 0.5f * (bp + sp);    // (+1,0,+1)
+        R.at<14>(pos) = 0.5f * (bp - sp);    // (-1,0,-1)
+        R.at<13>(pos) = 0.5f * (bm + sn);    // (+1,0,-1)
+        R.at<12>(pos) = 0.5f * (bm - sn);    // (-1,0,+1)
+    }
+    {
+        const float b = by + c.bzz, bp = b + c.byz, bm = b - c.byz;
+        const float sp = c.ay + c.az, sn = c.ay - c.az;
+        R.at<15>(pos) = 0.5f * (bp + sp);    // (0,+1,+1)
+        R.at<18>(pos) = 0.5f * (bp - sp);    // (0,-1,-1)
+        R.at<17>(pos) = 0.5f * (bm + sn);    // (0,+1,-1)
+        R.at<16>(pos) = 0.5f * (bm - sn);    // (0,-1,+1)
     }
 }
 
-// A halo position contributes only the directions that point into the tile:
-// one in-plane axis + two in-plane diagonals + one up + one down (edges), or one
-// in-plane diagonal (corners).  dir: 0 = x-1 column (+x), 1 = x+TX column (-x),
-// 2 = y-1 row (+y), 3 = y+TY row (-y), 4..7 = corners feeding 7, 8, 9, 10.
-__device__ __forceinline__ void build_halo(float* sm, int pos, int dir, const Coef& up, const Coef& mid,
-                                           const Coef& dn, bool s_up, bool s_mid, bool s_dn) {
+// A halo position writes only the directions that point into the tile:
+// dir 0 = x-1 column (+x), 1 = x+TX column (-x), 2 = y-1 row (+y),
+// 3 = y+TY row (-y), 4..7 = corners feeding 7, 8, 9, 10.
+__device__ __forceinline__ void build_halo(const Ring& R, int pos, int dir, const Coef& c) {
     switch (dir) {
         case 0:
-            if (!s_mid) { sm[slot(1) + pos] = mid.fpost<1>(); sm[slot(7) + pos] = mid.fpost<7>();
-                          sm[slot(9) + pos] = mid.fpost<9>(); }
-            if (!s_up) sm[slot(11) + pos] = up.fpost<11>();
-            if (!s_dn) sm[slot(13) + pos] = dn.fpost<13>();
+            R.at<1>(pos) = c.fpost<1>(); R.at<7>(pos) = c.fpost<7>(); R.at<9>(pos) = c.fpost<9>();
+            R.at<11>(pos) = c.fpost<11>(); R.at<13>(pos) = c.fpost<13>();
             break;
         case 1:
-            if (!s_mid) { sm[slot(2) + pos] = mid.fpost<2>(); sm[slot(8) + pos] = mid.fpost<8>();
-                          sm[slot(10) + pos] = mid.fpost<10>(); }
-            if (!s_up) sm[slot(12) + pos] = up.fpost<12>();
-            if (!s_dn) sm[slot(14) + pos] = dn.fpost<14>();
+            R.at<2>(pos) = c.fpost<2>(); R.at<8>(pos) = c.fpost<8>(); R.at<10>(pos) = c.fpost<10>();
+            R.at<12>(pos) = c.fpost<12>(); R.at<14>(pos) = c.fpost<14>();
             break;
         case 2:
-            if (!s_mid) { sm[slot(3) + pos] = mid.fpost<3>(); sm[slot(7) + pos] = mid.fpost<7>();
-                          sm[slot(8) + pos] = mid.fpost<8>(); }
-            if (!s_up) sm[slot(15) + pos] = up.fpost<15>();
-            if (!s_dn) sm[slot(17) + pos] = dn.fpost<17>();
+            R.at<3>(pos) = c.fpost<3>(); R.at<7>(pos) = c.fpost<7>(); R.at<8>(pos) = c.fpost<8>();
+            R.at<15>(pos) = c.fpost<15>(); R.at<17>(pos) = c.fpost<17>();
             break;
         case 3:
-            if (!s_mid) { sm[slot(4) + pos] = mid.fpost<4>(); sm[slot(9) + pos] = mid.fpost<9>();
-                          sm[slot(10) + pos] = mid.fpost<10>(); }
-            if (!s_up) sm[slot(16) + pos] = up.fpost<16>();
-            if (!s_dn) sm[slot(18) + pos] = dn.fpost<18>();
+            R.at<4>(pos) = c.fpost<4>(); R.at<9>(pos) = c.fpost<9>(); R.at<10>(pos) = c.fpost<10>();
+            R.at<16>(pos) = c.fpost<16>(); R.at<18>(pos) = c.fpost<18>();
             break;
-        case 4: if (!s_mid) sm[slot(7) + pos] = mid.fpost<7>(); break;
-        case 5: if (!s_mid) sm[slot(8) + pos] = mid.fpost<8>(); break;
-        case 6: if (!s_mid) sm[slot(9) + pos] = mid.fpost<9>(); break;
-        case 7: if (!s_mid) sm[slot(10) + pos] = mid.fpost<10>(); break;
+        case 4: R.at<7>(pos) = c.fpost<7>(); break;
+        case 5: R.at<8>(pos) = c.fpost<8>(); break;
+        case 6: R.at<9>(pos) = c.fpost<9>(); break;
+        case 7: R.at<10>(pos) = c.fpost<10>(); break;
         default: break;
     }
 }
 
 template <class T, bool STATS>
-__global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
+__global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
     extern __shared__ float sm[];
     const T* __restrict__ m = static_cast<const T*>(p.m);
     T* __restrict__ mn = static_cast<T*>(p.mn);
@@ -256,7 +252,7 @@ __global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
     uint32_t freg = 0;
     auto load = [&](int z) {
         if (!exists) return;
-        const int zz = ((z % nz) + nz) % nz;
+        const int zz = z < 0 ? z + nz : (z >= nz ? z - nz : z);
         const int64_t id = (int64_t)zz * plane + coff;
         const T* ptr = m + id;
 #pragma unroll
@@ -266,49 +262,62 @@ __global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
         }
         freg = flags ? flags[id] : 0u;
     };
-    // rebuild coefficients and flag bytes of this position for planes z-1, z, z+1
-    Coef C0, C1, C2;
-    uint32_t F0, F1, F2;
-    load(z0 - 1);
-    C0.set(mreg, omw); F0 = freg;
-    load(z0);
-    C1.set(mreg, omw); F1 = freg;
-    load(z0 + 1);
-    C2.set(mreg, omw); F2 = freg;
-    if (z0 + 2 <= z1) load(z0 + 2);
+    // the moments of plane pz are in mreg/freg: write the populations leaving it
+    // (a solid cell writes none; its slots are filled by its fluid neighbours)
+    auto arrive = [&](int pz) {
+        if (exists && !(freg & F_SOLID)) {
+            Coef c;
+            c.set(mreg, omw);
+            const Ring R(sm, pz);
+            if (dir == -1) build_tile_cell(R, pos, c);
+            else build_halo(R, pos, dir, c);
+        }
+    };
 
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
 
+    load(z0 - 1);
+    arrive(z0 - 1);
+    load(z0);
+    arrive(z0);
+    uint32_t fcur = freg;          // this position's flags in the plane being gathered
+    load(z0 + 1);
+
     for (int z = z0; z < z1; ++z) {
-        // 1. populations into the tile: a solid cell contributes nothing (its
-        //    slots are the ones its fluid neighbours fill in step 2)
-        if (exists) {
-            if (dir == -1) build_tile_cell(sm, pos, C0, C1, C2, F0 & F_SOLID, F1 & F_SOLID, F2 & F_SOLID);
-            else build_halo(sm, pos, dir, C0, C1, C2, F0 & F_SOLID, F1 & F_SOLID, F2 & F_SOLID);
-        }
+        // 1. plane z+1 arrives (its moments were loaded one iteration ago); z+2 is requested
+        arrive(z + 1);
+        const uint32_t fnext = freg;
+        if (z + 2 <= z1) load(z + 2);
         // 2. a link that does not stream: the cell writes the replacement into the
         //    slot of the source it would have gathered from (read by nobody else)
-        if (owner && (F1 & F_SPECIAL)) {
+        if (owner && (fcur & F_SPECIAL)) {
             const int64_t id = (int64_t)z * plane + coff;
             const uint32_t lk = p.links[id];
-            float rho_own = 0.f;
-            if (p.duct && (gx == 0)) rho_own = MomStore<T>::ld(m + id, 0, r0);
+            float own[10];
+            {
+                const T* ptr = m + id;
+#pragma unroll
+                for (int c = 0; c < 10; ++c) { own[c] = MomStore<T>::ld(ptr, c, r0); ptr += N; }
+            }
+            Coef oc;
+            oc.set(own, omw);
+            const Ring Rm(sm, z - 1), Rz(sm, z), Rp(sm, z + 1);
             static_for<1, 19>([&](auto qi) {
                 constexpr int q = decltype(qi)::value;
                 if ((lk >> opp(q)) & 1u) {
                     const int xs = gx - cx(q);
                     float v;
                     if (p.duct && xs < 0) {
-                        v = feq_ref(q, rho_own, p.u_in, 0.f, 0.f);                      // inlet
+                        v = feq_ref(q, own[0], p.u_in, 0.f, 0.f);                      // inlet
                     } else if (p.duct && xs >= nx) {
-                        v = C1.template fpost<q>();                                        // outlet
+                        v = oc.template fpost<q>();                                       // outlet
                     } else {
                         // own post-collision population of direction bq comes back as q
                         // (home.cu:219-225); bq = opp(q), or the reference's table
                         constexpr int bt = opp(q), br = opp_tab(q);
-                        v = p.ref_bounce ? C1.template fpost<br>() : C1.template fpost<bt>();
+                        v = p.ref_bounce ? oc.template fpost<br>() : oc.template fpost<bt>();
                         if (STATS) {
                             const int bq = p.ref_bounce ? br : bt;
                             const int ys = ((gy - cy(q)) % ny + ny) % ny;
@@ -321,7 +330,9 @@ __global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
                             }
                         }
                     }
-                    sm[slot(q) + pos - cx(q) - HX * cy(q)] = v;
+                    // the source of q sits in plane z - c_z(q)
+                    const Ring& R = cz(q) > 0 ? Rm : (cz(q) == 0 ? Rz : Rp);
+                    R.template at<q>(pos - cx(q) - HX * cy(q)) = v;
                 }
             });
         }
@@ -330,15 +341,17 @@ __global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
         if (owner) {
             const int64_t id = (int64_t)z * plane + coff;
             T* op = mn + id;
-            if (F1 & F_SOLID) {
+            if (fcur & F_SOLID) {
                 MomStore<T>::st(op, 0, r0, 1.f);
 #pragma unroll
                 for (int c = 1; c < 10; ++c) MomStore<T>::st(op + c * N, c, r0, 0.f);
             } else {
+                const Ring Rm(sm, z - 1), Rz(sm, z), Rp(sm, z + 1);
                 float fq[19];
                 static_for<0, 19>([&](auto qi) {
                     constexpr int q = decltype(qi)::value;
-                    fq[q] = sm[slot(q) + pos - cx(q) - HX * cy(q)];
+                    const Ring& R = cz(q) > 0 ? Rm : (cz(q) == 0 ? Rz : Rp);
+                    fq[q] = R.template at<q>(pos - cx(q) - HX * cy(q));
                 });
                 // moments of the gathered populations (home.cu:238-273), opposite pairs first
                 const float s1 = fq[1] + fq[2], d1 = fq[1] - fq[2];
@@ -379,13 +392,8 @@ __global__ void __launch_bounds__(NT, 2) home_step(HomeParams p) {
                 }
             }
         }
+        fcur = fnext;
         __syncthreads();
-        if (z + 1 < z1) {
-            C0 = C1; F0 = F1;
-            C1 = C2; F1 = F2;
-            C2.set(mreg, omw); F2 = freg;       // plane z+2, loaded one iteration ago
-            if (z + 3 <= z1) load(z + 3);
-        }
     }
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }

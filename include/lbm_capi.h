@@ -188,6 +188,20 @@ int lbm_set_macro_output(lbm_solver* s, int enable);
  * same result as lbm_step.  Invalidated by any setter. */
 int lbm_step_graph(lbm_solver* s, int substeps);
 
+/* FP64 sums of DEVICE fields rho, ux, uy, uz of n cells into the DEVICE array
+ * d_out[LBM_NSTAT]: MASS, KE and MOM_X/Y/Z as lbm_get_stats defines them (the
+ * drag slots are 0).  Cells whose d_mask byte is nonzero are left out (d_mask
+ * may be NULL).  Asynchronous on `stream` (NULL: the default stream).
+ * Allocates no memory: its partial sums live in a fixed 2 MiB __device__
+ * array, so it suits callers that may not allocate while they run.  Limits:
+ * n <= 268,435,456 cells (LBM_ERR_SIZE beyond); calls that overlap in time on
+ * one device race on the shared array and must be ordered by the caller; the
+ * first call on each device does a one-time address lookup and should come
+ * before any stream capture.  No counterpart in the reference (it sums on the
+ * host, src/bench/main_taylor_green.cpp:157-182). */
+int lbm_macro_stats_static(const float* d_rho, const float* d_ux, const float* d_uy, const float* d_uz,
+                           const uint8_t* d_mask, int64_t n, double* d_out, void* stream);
+
 /* ---- geometry (host in, host out) ------------------------------------- */
 
 /* STL loader: ASCII when the file starts with "solid" (falls back to binary

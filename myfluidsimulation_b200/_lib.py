@@ -73,6 +73,7 @@ _PROTOS = [
     ("lbm_enable_stats", C.c_int, [_P, C.c_int]),
     ("lbm_get_stats", C.c_int, [_P, _P]),
     ("lbm_set_macro_output", C.c_int, [_P, C.c_int]),
+    ("lbm_macro_stats_static", C.c_int, [_P, _P, _P, _P, _P, C.c_int64, _P, _P]),
     ("lbm_load_stl", C.c_int, [C.c_char_p, C.POINTER(_P), C.POINTER(C.c_int64), _P]),
     ("lbm_free", None, [_P]),
     ("lbm_voxelize", C.c_int, [_P, C.c_int64, _P, C.POINTER(VoxelParams), _P]),

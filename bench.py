@@ -369,7 +369,7 @@ def main():
                         "kernel_us": r["kernel_us"],
                         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                                      "frac": round(achieved / peak, 4),
-                                     "traffic": None if tr is None else round(tr * N / 1e6, 2),
+                                     "traffic": None if tr is None else int(round(tr * N)),
                                      "kernel": KERNEL[mth], "bytes_per_cell": BYTES[mth]},
                         "drag": [round(x, 6) for x in r["drag_last"]], "mass": round(r["mass"], 3),
                         "launches": r["launches"]}

@@ -220,7 +220,7 @@ struct Nbr {
 // Odd step: one cell per thread, rows of blockDim.x cells per block iteration.
 // ---------------------------------------------------------------------------
 template <class ST, bool MASK, int MODE, class IDX>
-__global__ void __launch_bounds__(256, 3) aa_odd(AAParams p) {
+__global__ void __launch_bounds__(256, MASK ? 4 : 3) aa_odd(AAParams p) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     using T = typename ST::T;
     T* __restrict__ f = static_cast<T*>(p.f);

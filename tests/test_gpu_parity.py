@@ -87,6 +87,8 @@ CASES = [
     ((24, 10, 12), 0.56, 20, True, (1e-5, 0, 0)),
     ((17, 9, 11), 0.7, 15, True, (2e-6, -1e-6, 3e-6)),   # odd sizes: scalar even path, wraps
     ((32, 8, 1), 0.6, 9, True, (0, 0, 0)),               # a single z plane
+    ((136, 5, 4), 0.6, 7, True, (1e-5, 0, 0)),           # 128-cell staged tiles, a partial second tile
+    ((260, 3, 3), 0.58, 6, False, (0, 2e-6, 0)),         # three tiles per row, periodic x wrap
 ]
 
 
@@ -170,14 +172,14 @@ def test_home_vs_oracle(gpu, oracle, dims, tau, steps, with_mask, force, bounce)
     assert rl2(g["macros"][0], m[0]) < TOL_F
 
 
+@pytest.mark.parametrize("dims", [(40, 18, 14), (136, 10, 8)])
 @pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HYBRID, METHOD_HOME])
-def test_duct_vs_oracle(gpu, oracle, method):
+def test_duct_vs_oracle(gpu, oracle, method, dims):
     """Velocity inlet / zero-gradient outlet / wall cells / obstacle; drag of the last step."""
-    dims = (40, 18, 14)
     nx, ny, nz = dims
     sphere = np.zeros((nz, ny, nx), np.uint8)
     Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
-    sphere[(X - 12) ** 2 + (Y - 9) ** 2 + (Z - 7) ** 2 <= 9] = 1
+    sphere[(X - 12) ** 2 + (Y - ny // 2) ** 2 + (Z - nz // 2) ** 2 <= 9] = 1
     mask = W.duct_mask(nx, ny, nz, sphere)
     rho = np.ones((nz, ny, nx), np.float32)
     u = np.full((nz, ny, nx), 0.04, np.float32)

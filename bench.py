@@ -299,6 +299,67 @@ def reference_arm(args, torch, rank, world):
     print(json.dumps(base))
 
 
+def precision_study(args, torch):
+    """512^3 periodic Taylor-Green vortex (tau 0.51, u0 0.05, k 2pi/512): MLUPS of
+    FP32 / F16 / BF16 storage for Legacy and HOME, and the kinetic-energy decay
+    of each form against the FP32 run of the same method after --tgv-steps steps."""
+    from myfluidsimulation_b200.solvers import METHOD_HOME, METHOD_LEGACY, STORE_BF16, STORE_F16, STORE_F32, Solver
+    n = args.tgv_n
+    N = n ** 3
+    steps = args.tgv_steps
+    st = torch.cuda.current_stream()
+    # the analytic field at cell centres, built on the device in FP64 and cast
+    k = 2 * math.pi / n
+    c = (torch.arange(n, device="cuda", dtype=torch.float64) + 0.5) * k
+    z, y, x = c.view(n, 1, 1), c.view(1, n, 1), c.view(1, 1, n)
+    u = (0.05 * torch.sin(x) * torch.cos(y) * torch.cos(z)).float().contiguous()
+    v = (-0.05 * torch.cos(x) * torch.sin(y) * torch.cos(z)).float().contiguous()
+    w = torch.zeros_like(u)
+    rho = (1.0 + 3.0 * (0.05 ** 2 / 16.0) * (torch.cos(2 * x) + torch.cos(2 * y)) * (torch.cos(2 * z) + 2.0)).float().contiguous()
+    del c, z, y, x
+    out = {}
+    bytes_cell = {("legacy", STORE_F32): 152, ("legacy", STORE_F16): 76, ("legacy", STORE_BF16): 76,
+                  ("home", STORE_F32): 80, ("home", STORE_F16): 40, ("home", STORE_BF16): 40}
+    peak, _ = measured_peaks()
+    for mname, m in (("legacy", METHOD_LEGACY), ("home", METHOD_HOME)):
+        ref_ke = None
+        for sname, sto in (("f32", STORE_F32), ("f16", STORE_F16), ("bf16", STORE_BF16)):
+            s = Solver(n, n, n, 0.51, method=m, storage=sto, stream=st.cuda_stream)
+            s.reinit_from_macro(rho, u, v, w)
+            s.set_macro_output(False)
+            for _ in range(4):
+                s.step(1)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(st)
+            s.step(args.steps)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            mlups = N * args.steps / (ms * 1e-3) / 1e6
+            # accuracy run from the initial field
+            s.reinit_from_macro(rho, u, v, w)
+            s.enable_stats(True)
+            s.step(1)
+            ke0 = s.stats()["ke_sum"] / N
+            s.step(steps - 1)
+            ke = s.stats()["ke_sum"] / N
+            s.close()
+            if sto == STORE_F32:
+                ref_ke = ke
+            b = bytes_cell[(mname, sto)]
+            out[f"{mname}_{sname}"] = {
+                "mlups": round(mlups, 1), "us_per_step": round(ms * 1e3 / args.steps, 1),
+                "roofline_frac": round(N * b / (ms * 1e-3 / args.steps) / 1e9 / peak, 4), "bytes_per_cell": b,
+                "ke_decay": ke / ke0, "ke_rel_err_vs_f32": abs(ke - ref_ke) / ref_ke}
+        for sname in ("f16", "bf16"):
+            out[f"{mname}_{sname}"]["speedup_vs_f32"] = round(
+                out[f"{mname}_{sname}"]["mlups"] / out[f"{mname}_f32"]["mlups"], 3)
+    print(json.dumps({"study": "precision", "workload": f"TGV {n}^3 periodic, tau 0.51, u0 0.05, "
+                      f"{args.steps} timed steps, KE after {steps} steps", "results": out}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -309,6 +370,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default=None,
                     help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
+    ap.add_argument("--study", default=None, choices=["precision"],
+                    help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage")
+    ap.add_argument("--tgv-n", type=int, default=512)
+    ap.add_argument("--tgv-steps", type=int, default=2000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -332,6 +397,9 @@ def main():
 
     import myfluidsimulation_b200 as P
     P.lib()
+    if args.study == "precision":
+        precision_study(args, torch)
+        return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)
     if args.profile:

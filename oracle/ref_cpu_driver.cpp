@@ -80,4 +80,30 @@ void ref_band(const uint8_t* mask, int nx, int ny, int nz, int d0, int32_t* dist
     for (size_t i = 0; i < N; ++i) { dist_out[i] = dist[i]; legacy_out[i] = leg[i]; }
 }
 
+// parse_common_args (sim_common.hpp:115-192) on an argv, printed as the
+// key=value lines that the library's command-line tools print with
+// --print-config.  Returns the length written, or -1 when the reference's
+// parser throws (std::stoi/stof on a non-number).
+int ref_parse_common_args(int argc, char** argv, int hybrid, char* out, int cap) {
+    DomainConfig dom;
+    ObstacleConfig obs;
+    RunConfig run;
+    HybridConfig hyb;
+    try {
+        parse_common_args(argc, argv, dom, obs, run, hybrid ? &hyb : nullptr);
+    } catch (...) {
+        return -1;
+    }
+    return std::snprintf(
+        out, (size_t)cap,
+        "nx=%d\nny=%d\nnz=%d\ntau=%.9g\nforce=%.9g,%.9g,%.9g\n"
+        "stl=%s\nvoxel_scale=%.9g\nvoxel_translate=%.9g,%.9g,%.9g\namr_factor=%d\namr_threshold=%.9g\n"
+        "steps=%d\nsubsteps=%d\nvtk_dir=%s\nvtk_every=%d\ninit=%s\namp=%.9g\nsigma=%.9g\n"
+        "center=%.9g,%.9g,%.9g\nslab_axis=%d\nslab_center=%.9g\nslab_width=%.9g\nband_d0=%d\n",
+        dom.Nx, dom.Ny, dom.Nz, dom.tau, dom.fx, dom.fy, dom.fz, obs.stlPath.c_str(), obs.uniformScale,
+        obs.translateX, obs.translateY, obs.translateZ, obs.amrFactor, obs.amrThreshold, run.steps, run.substeps,
+        run.vtkDir.c_str(), run.vtkEvery, run.initMode.c_str(), run.amp, run.sigma, run.cx, run.cy, run.cz,
+        run.slabAxis, run.slabCenter, run.slabWidth, hyb.bandD0);
+}
+
 }  // extern "C"

@@ -1,0 +1,102 @@
+"""Storage precision against the FP64 oracle on the 64^3 Taylor-Green vortex.
+
+Workload: 3-D TGV, 64^3 fully periodic, tau=0.6, rho0=1, u0=0.05, k=2*pi/64,
+populations (or HOME's moments) initialised at equilibrium from the analytic
+field at cell centres; 1000 steps with the kinetic energy (mean of |u|^2/2
+over all cells, FP64 reduction on the GPU) recorded every 10 steps.
+
+FP32 storage must stay within 1e-5 relative L2 of the FP64 oracle in the
+fields and the energy curve.  F16/BF16 store the shifted value f_q - w_q*rho0
+(HOME: rho - rho0, u, S) with FP32 arithmetic; their bound is on the relative
+error of the kinetic energy (F16: 1e-3) and is reported for the fields.
+"""
+import numpy as np
+import pytest
+
+from myfluidsimulation_b200 import workloads as W
+from myfluidsimulation_b200.solvers import METHOD_HOME, METHOD_LEGACY, STORE_BF16, STORE_F16, STORE_F32, Solver
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (64, 64, 64)
+TAU, U0 = 0.6, 0.05
+STEPS, EVERY = 1000, 10
+
+TOL_FIELD_F32 = 1e-5
+TOL_KE_F32 = 1e-5
+# relative KE error bounds and field bounds of the narrow forms
+TOL_KE = {STORE_F16: 1e-3, STORE_BF16: 2e-2}
+TOL_FIELD = {STORE_F16: 2e-3, STORE_BF16: 5e-2}
+
+
+def rl2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def fields():
+    return W.taylor_green_3d(*DIMS, U0)
+
+
+@pytest.fixture(scope="module")
+def reference_curves(oracle):
+    """FP64 oracle: KE every EVERY steps and the final macro fields, both methods."""
+    rho, u, v, w = fields()
+    N = rho.size
+    out = {}
+    f = oracle.reinit_eq(rho, u, v, w)
+    ke, mac = [], None
+    for _ in range(STEPS // EVERY):
+        f, r, ux, uy, uz, _ = oracle.bgk_run(f, None, EVERY, TAU)
+        ke.append(0.5 * float(np.sum(ux * ux + uy * uy + uz * uz)) / N)
+        mac = (r, ux, uy, uz)
+    out[METHOD_LEGACY] = (np.array(ke), mac)
+    m = np.zeros((10,) + rho.shape)
+    m[0], m[1], m[2], m[3] = rho, u, v, w
+    ke = []
+    for _ in range(STEPS // EVERY):
+        m, _ = oracle.home_run(m, None, EVERY, TAU)
+        ke.append(0.5 * float(np.sum(m[1] ** 2 + m[2] ** 2 + m[3] ** 2)) / N)
+    out[METHOD_HOME] = (np.array(ke), (m[0], m[1], m[2], m[3]))
+    return out
+
+
+def gpu_curve(method, storage):
+    rho, u, v, w = fields()
+    N = rho.size
+    s = Solver(*DIMS, TAU, method=method, storage=storage)
+    s.reinit_from_host(rho, u, v, w)
+    s.enable_stats(True)
+    ke = []
+    for _ in range(STEPS // EVERY):
+        s.step(EVERY)
+        ke.append(s.stats()["ke_sum"] / N)
+    mac = s.macros()
+    s.close()
+    return np.array(ke), mac
+
+
+@pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HOME])
+def test_tgv64_fp32_within_1e5_of_fp64(gpu, reference_curves, method):
+    ke_ref, mac_ref = reference_curves[method]
+    ke, mac = gpu_curve(method, STORE_F32)
+    e_ke = float(np.max(np.abs(ke - ke_ref) / ke_ref))
+    e_u = rl2(np.stack(mac[1:]), np.stack(mac_ref[1:]))
+    e_r = rl2(mac[0] - 1.0, mac_ref[0] - 1.0)
+    print(f"method {method} F32: KE max rel err {e_ke:.3e}, u rel L2 {e_u:.3e}, (rho-1) rel L2 {e_r:.3e}, "
+          f"KE decay {ke_ref[-1] / ke_ref[0]:.4f}")
+    assert e_ke < TOL_KE_F32
+    assert e_u < TOL_FIELD_F32
+
+
+@pytest.mark.parametrize("storage", [STORE_F16, STORE_BF16])
+@pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HOME])
+def test_tgv64_narrow_storage_error(gpu, reference_curves, method, storage):
+    ke_ref, mac_ref = reference_curves[method]
+    ke, mac = gpu_curve(method, storage)
+    e_ke = float(np.max(np.abs(ke - ke_ref) / ke_ref))
+    e_u = rl2(np.stack(mac[1:]), np.stack(mac_ref[1:]))
+    print(f"method {method} storage {storage}: KE max rel err {e_ke:.3e}, u rel L2 {e_u:.3e}")
+    assert e_ke < TOL_KE[storage]
+    assert e_u < TOL_FIELD[storage]

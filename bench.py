@@ -360,6 +360,107 @@ def precision_study(args, torch):
                       f"{args.steps} timed steps, KE after {steps} steps", "results": out}))
 
 
+def batch_instances(count=64, seed=20261203):
+    """The batched Hybrid(B0) sweep: `count` duct-with-sphere instances drawn from a
+    seeded numpy generator: nx in {64,80,..,192}, ny, nz in {32,48,..,96}, B0 in
+    {0,1,2,3,4,6}, tau uniform in [0.51, 0.8], sphere radius 0.15 min(ny,nz) at
+    x = nx/4 (y, z centred), inlet u = 0.04."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nx = int(rng.choice(np.arange(64, 193, 16)))
+        ny = int(rng.choice(np.arange(32, 97, 16)))
+        nz = int(rng.choice(np.arange(32, 97, 16)))
+        out.append({"dims": (nx, ny, nz), "b0": int(rng.choice([0, 1, 2, 3, 4, 6])),
+                    "tau": float(rng.uniform(0.51, 0.8)), "radius": 0.15 * min(ny, nz),
+                    "center": (nx / 4, ny / 2, nz / 2), "u_in": 0.04})
+    return out
+
+
+def batch_study(args, torch):
+    """64 uneven Hybrid(B0) duct instances: one persistent launch per step over all
+    of them (autotuned, graph-replayed) against stepping them one by one."""
+    from myfluidsimulation_b200 import geometry as G
+    from myfluidsimulation_b200 import workloads as W
+    from myfluidsimulation_b200.solvers import BC_DUCT, METHOD_HYBRID, Batch, Solver
+    st = torch.cuda.current_stream()
+    specs = batch_instances(args.batch_count)
+    steps = args.batch_steps
+
+    def make_all():
+        solvers = []
+        for sp in specs:
+            nx, ny, nz = sp["dims"]
+            tris, scale, tr = W.duct_sphere_mesh(nx, ny, nz, sp["radius"], sp["center"], levels=3)
+            sph = G.voxelize_mesh_to_mask(G.mesh_from_triangles(tris), G.VoxelParams(nx, ny, nz, scale, tr))
+            mask = W.duct_mask(nx, ny, nz, sph)
+            s = Solver(nx, ny, nz, sp["tau"], method=METHOD_HYBRID, bc=BC_DUCT, inlet_u=sp["u_in"],
+                       stream=st.cuda_stream)
+            s.set_solid_mask(mask)
+            s.build_band(sp["b0"])
+            u = np.full((nz, ny, nx), sp["u_in"], np.float32)
+            u[mask != 0] = 0
+            sp["u0"] = u
+            s.reinit_from_host(np.ones((nz, ny, nx), np.float32), u, None, None)
+            s.set_macro_output(False)
+            solvers.append(s)
+        return solvers
+
+    cells = sum(int(np.prod(sp["dims"])) for sp in specs)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    # one by one: every instance advanced through its own captured graph
+    solvers = make_all()
+    for s in solvers:
+        s.step_graph(50)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record(st)
+    for s in solvers:
+        for _ in range(steps // 50):
+            s.step_graph(50)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms_seq = e0.elapsed_time(e1)
+    drag_seq = []
+    for s in solvers:
+        s.enable_stats(True)
+        s.step(2)
+        drag_seq.append(s.stats()["drag_x"])
+        s.close()
+    # batched
+    solvers = make_all()
+    b = Batch(solvers, stream=st.cuda_stream)
+    tuning = b.tune(2)
+    for s, sp in zip(solvers, specs):   # restart from the initial state after tuning
+        nx, ny, nz = sp["dims"]
+        s.reinit_from_host(np.ones((nz, ny, nx), np.float32), sp["u0"], None, None)
+    b.refresh()
+    b.step(50)
+    torch.cuda.synchronize()
+    e0, e1 = ev(), ev()
+    e0.record(st)
+    for _ in range(steps // 50):
+        b.step(50)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
+    b.enable_stats(True)
+    b.step(2)
+    drag_b = b.stats()[:, 2]
+    b.close()
+    for s in solvers:
+        s.close()
+    done = cells * (steps // 50) * 50
+    print(json.dumps({"study": "batch", "instances": len(specs), "cells": cells, "steps": (steps // 50) * 50,
+                      "batched": {"mlups": round(done / (ms_b * 1e-3) / 1e6, 1), "ms": round(ms_b, 2),
+                                  "launch": "one persistent launch per step, graph-replayed 50 at a time",
+                                  "tuning": tuning},
+                      "one_by_one": {"mlups": round(done / (ms_seq * 1e-3) / 1e6, 1), "ms": round(ms_seq, 2)},
+                      "drag_x_batched": [round(float(d), 6) for d in drag_b],
+                      "drag_x_max_abs_diff_vs_one_by_one": float(np.max(np.abs(np.array(drag_seq) - drag_b))),
+                      "b0": [sp["b0"] for sp in specs], "dims": [sp["dims"] for sp in specs]}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,8 +471,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default=None,
                     help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
-    ap.add_argument("--study", default=None, choices=["precision"],
-                    help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage")
+    ap.add_argument("--study", default=None, choices=["precision", "batch"],
+                    help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage; "
+                         "batch: 64 uneven Hybrid(B0) ducts in one persistent launch per step")
+    ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--tgv-n", type=int, default=512)
     ap.add_argument("--tgv-steps", type=int, default=2000)
     args = ap.parse_args()
@@ -399,6 +503,9 @@ def main():
     P.lib()
     if args.study == "precision":
         precision_study(args, torch)
+        return
+    if args.study == "batch":
+        batch_study(args, torch)
         return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)

@@ -202,6 +202,47 @@ int lbm_step_graph(lbm_solver* s, int substeps);
 int lbm_macro_stats_static(const float* d_rho, const float* d_ux, const float* d_uy, const float* d_uz,
                            const uint8_t* d_mask, int64_t n, double* d_out, void* stream);
 
+/* ---- batched instances ------------------------------------------------- */
+
+/* Many independent Legacy/Hybrid solvers (FP32 populations, halfway
+ * bounce-back, even cell counts, any sizes, rates, bands and boundaries)
+ * advanced together: every substep is ONE persistent launch over all of them,
+ * and a multi-step lbm_batch_step is replayed from a captured CUDA graph.  No
+ * reference counterpart: the reference runs one solver per process and times
+ * each B0 of its sweep separately (src/main_compare.cpp:511-699). */
+typedef struct lbm_batch lbm_batch;
+/* Launch shape of the batched step, chosen by lbm_batch_tune (or set). */
+typedef struct lbm_batch_tuning {
+    int32_t threads;         /* threads per block (128 or 256) */
+    int32_t blocks_per_sm;   /* persistent blocks per SM */
+    int32_t even_unit;       /* two-cell vectors per work unit of the local step */
+    int32_t odd_unit;        /* row segments (of `threads` cells) per unit of the neighbour step */
+    float us_per_step;       /* measured by lbm_batch_tune: mean of one even + one odd launch / 2 */
+} lbm_batch_tuning;
+
+/* The solvers must be at the same step parity; they stay owned by the caller,
+ * must outlive the batch, and may be read (lbm_get_state, lbm_get_macros)
+ * between batch steps.  The batch keeps a snapshot of each solver's settings
+ * (mask, band, rates, force, boundary) taken here or by lbm_batch_refresh;
+ * after stepping or reinitialising an instance on its own, call
+ * lbm_batch_refresh (lbm_batch_step refuses instances out of step). */
+int lbm_batch_create(lbm_solver* const* solvers, int32_t n, void* stream, lbm_batch** out);
+int lbm_batch_refresh(lbm_batch* b);
+int lbm_batch_destroy(lbm_batch* b);
+/* Times every candidate launch shape for `trial_pairs` even+odd step pairs on
+ * the batch's own instances (which therefore advance by those steps) and keeps
+ * the fastest; out (may be NULL) receives it. */
+int lbm_batch_tune(lbm_batch* b, int32_t trial_pairs, lbm_batch_tuning* out);
+int lbm_batch_set_tuning(lbm_batch* b, const lbm_batch_tuning* t);
+int lbm_batch_get_tuning(lbm_batch* b, lbm_batch_tuning* out);
+/* Advances every instance by `substeps` steps, asynchronously. */
+int lbm_batch_step(lbm_batch* b, int32_t substeps);
+int lbm_batch_synchronize(lbm_batch* b);
+/* Statistics (and macro fields) of the last substep of every lbm_batch_step. */
+int lbm_batch_enable_stats(lbm_batch* b, int enable);
+/* Synchronises and copies n x LBM_NSTAT doubles (instance-major). */
+int lbm_batch_get_stats(lbm_batch* b, double* out);
+
 /* ---- geometry (host in, host out) ------------------------------------- */
 
 /* STL loader: ASCII when the file starts with "solid" (falls back to binary

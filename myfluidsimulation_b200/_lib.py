@@ -45,6 +45,11 @@ class VoxelParams(C.Structure):
                 ("translate", C.c_float * 3), ("refine", C.c_int32), ("coverage_threshold", C.c_float)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("even_unit", C.c_int32),
+                ("odd_unit", C.c_int32), ("us_per_step", C.c_float)]
+
+
 # (name, restype, argtypes)
 _P = C.c_void_p
 _PROTOS = [
@@ -74,6 +79,16 @@ _PROTOS = [
     ("lbm_get_stats", C.c_int, [_P, _P]),
     ("lbm_set_macro_output", C.c_int, [_P, C.c_int]),
     ("lbm_macro_stats_static", C.c_int, [_P, _P, _P, _P, _P, C.c_int64, _P, _P]),
+    ("lbm_batch_create", C.c_int, [C.POINTER(_P), C.c_int32, _P, C.POINTER(_P)]),
+    ("lbm_batch_refresh", C.c_int, [_P]),
+    ("lbm_batch_destroy", C.c_int, [_P]),
+    ("lbm_batch_tune", C.c_int, [_P, C.c_int32, C.POINTER(BatchTuning)]),
+    ("lbm_batch_set_tuning", C.c_int, [_P, C.POINTER(BatchTuning)]),
+    ("lbm_batch_get_tuning", C.c_int, [_P, C.POINTER(BatchTuning)]),
+    ("lbm_batch_step", C.c_int, [_P, C.c_int32]),
+    ("lbm_batch_synchronize", C.c_int, [_P]),
+    ("lbm_batch_enable_stats", C.c_int, [_P, C.c_int]),
+    ("lbm_batch_get_stats", C.c_int, [_P, _P]),
     ("lbm_load_stl", C.c_int, [C.c_char_p, C.POINTER(_P), C.POINTER(C.c_int64), _P]),
     ("lbm_free", None, [_P]),
     ("lbm_voxelize", C.c_int, [_P, C.c_int64, _P, C.POINTER(VoxelParams), _P]),

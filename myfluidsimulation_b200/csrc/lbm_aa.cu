@@ -62,7 +62,8 @@ __device__ __forceinline__ Cell moments(const float (&f)[19], float fx, float fy
 // (The Hybrid's "HOME form" of hybrid.cu:148-152 is this with w = omega_shear.)
 __device__ __forceinline__ void collide(float (&f)[19], const Cell& c, float omega) {
     const float A = 1.0f - 1.5f * (c.ux * c.ux + c.uy * c.uy + c.uz * c.uz);
-    const float r0 = (1.0f / 3.0f) * c.r, r1 = (1.0f / 18.0f) * c.r, r2 = (1.0f / 36.0f) * c.r;
+    // w_q rho with the weights' own rounding compensated (mulk): no mass or momentum bias per step
+    const float r0 = mulk(c.r, K3_HI, K3_LO), r1 = mulk(c.r, K18_HI, K18_LO), r2 = mulk(c.r, K36_HI, K36_LO);
     auto pair = [&](int qp, int qm, float t, float wr) {
         const float sym = wr * fmaf(4.5f * t, t, A);
         const float asym = 3.0f * wr * t;
@@ -117,19 +118,15 @@ __device__ __forceinline__ float inlet_value(int q, float r, float kin) { return
 // Even step: local.  VEC consecutive cells per thread.
 // MODE 0: populations only; 1: + macro fields; 2: + macro fields + statistics
 // ---------------------------------------------------------------------------
+// One even-step unit: the VEC consecutive cells v*VEC .. v*VEC+VEC-1.
 template <class ST, bool MASK, int VEC, int MODE, class IDX>
-__global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
+__device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc)[NSTAT]) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     using T = typename ST::T;
     T* __restrict__ f = static_cast<T*>(p.f);
     const IDX N = (IDX)p.N;
-    const IDX nvec = N / VEC;
     const float kin = 1.0f + 3.0f * p.u_in + 3.0f * p.u_in * p.u_in;
-    double acc[NSTAT];
-#pragma unroll
-    for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-
-    for (IDX v = (IDX)blockIdx.x * blockDim.x + threadIdx.x; v < nvec; v += (IDX)gridDim.x * blockDim.x) {
+    {
         const IDX id = v * VEC;
         float a[19][VEC];
 #pragma unroll
@@ -190,6 +187,17 @@ __global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
             stv<StoreF32, VEC>(p.uz + id, 0, 0.f, mw);
         }
     }
+}
+
+template <class ST, bool MASK, int VEC, int MODE, class IDX>
+__global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
+    constexpr bool STATS = MODE == 2;
+    const IDX nvec = (IDX)p.N / VEC;
+    double acc[NSTAT];
+#pragma unroll
+    for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
+    for (IDX v = (IDX)blockIdx.x * blockDim.x + threadIdx.x; v < nvec; v += (IDX)gridDim.x * blockDim.x)
+        even_unit<ST, MASK, VEC, MODE, IDX>(p, v, acc);
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }
 
@@ -217,34 +225,25 @@ struct Nbr {
 };
 
 // ---------------------------------------------------------------------------
-// Odd step: one cell per thread, rows of blockDim.x cells per block iteration.
+// Odd step
 // ---------------------------------------------------------------------------
+// One odd-step cell: x of row `row` (= z*ny + y).
 template <class ST, bool MASK, int MODE, class IDX>
-__global__ void __launch_bounds__(256, MASK ? 4 : 3) aa_odd(AAParams p) {
+__device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, double (&acc)[NSTAT]) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     using T = typename ST::T;
     T* __restrict__ f = static_cast<T*>(p.f);
     const IDX N = (IDX)p.N;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
-    const int bx = blockDim.x;
-    const int segs = (nx + bx - 1) / bx;
-    const IDX total = (IDX)segs * ny * nz;
     const float kin = 1.0f + 3.0f * p.u_in + 3.0f * p.u_in * p.u_in;
-    double acc[NSTAT];
-#pragma unroll
-    for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-
-    for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
-        const IDX row = sg / segs;
-        const int x = (int)(sg - row * segs) * bx + threadIdx.x;
-        if (x >= nx) continue;
+    {
         const int y = (int)(row % ny);
         const int z = (int)(row / ny);
         const IDX id = row * nx + x;
         const uint32_t fl = MASK ? p.flags[id] : 0u;
         if (MASK && (fl & F_SOLID)) {
             if (MACRO) { p.rho[id] = 1.f; p.ux[id] = 0.f; p.uy[id] = 0.f; p.uz[id] = 0.f; }
-            continue;
+            return;
         }
         Nbr<IDX> nb;
         nb.init(x, y, z, nx, ny, nz);
@@ -280,6 +279,23 @@ __global__ void __launch_bounds__(256, MASK ? 4 : 3) aa_odd(AAParams p) {
             add_cell_stats(acc, m);
             if (MASK && (fl & F_TOUCH)) add_drag(acc, o, lk, p.flags, x, y, z, nx, ny, nz, p.duct);
         }
+    }
+}
+
+// Odd step: one cell per thread, rows of blockDim.x cells per block iteration.
+template <class ST, bool MASK, int MODE, class IDX>
+__global__ void __launch_bounds__(256, MASK ? 4 : 3) aa_odd(AAParams p) {
+    constexpr bool STATS = MODE == 2;
+    const int bx = blockDim.x;
+    const int segs = (p.nx + bx - 1) / bx;
+    const IDX total = (IDX)segs * p.ny * p.nz;
+    double acc[NSTAT];
+#pragma unroll
+    for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
+    for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
+        const IDX row = sg / segs;
+        const int x = (int)(sg - row * segs) * bx + threadIdx.x;
+        if (x < p.nx) odd_cell<ST, MASK, MODE, IDX>(p, row, x, acc);
     }
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }
@@ -347,7 +363,109 @@ cudaError_t launch_typed(const AAParams& p, int parity, LaunchCfg cfg, cudaStrea
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Batched step: many independent instances (each its own AAParams: grid,
+// populations, flags, rates, boundary) advanced by ONE persistent launch.  The
+// work is a list of units {instance, first, count, -}: even steps count
+// two-cell vectors, odd steps count row segments of blockDim.x cells.  Blocks
+// take units round-robin; with statistics each unit's FP64 sums go to its own
+// slot and batch_finalize adds the slots of each instance in order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void block_reduce_into(double (&acc)[NSTAT], double* out) {
+    __shared__ double red[32][NSTAT];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < NSTAT; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int k = 0; k < NSTAT; ++k) {
+            double v = lane < nw ? red[lane][k] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) out[k] = v;
+        }
+    }
+    __syncthreads();
+}
+
+template <class ST, int MODE>
+__global__ void __launch_bounds__(256, 2) aa_batch_even(const AAParams* __restrict__ inst, const int4* __restrict__ units,
+                                                     int nunits, double* __restrict__ partials) {
+    constexpr bool STATS = MODE == 2;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int4 w = units[u];
+        const AAParams p = inst[w.x];   // the fields the unit uses, in registers
+        double acc[NSTAT];
+#pragma unroll
+        for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
+        for (int v = w.y + threadIdx.x; v < w.y + w.z; v += blockDim.x)
+            even_unit<ST, true, 2, MODE, uint32_t>(p, (uint32_t)v, acc);
+        if constexpr (STATS) block_reduce_into(acc, partials + (size_t)u * NSTAT);
+    }
+}
+
+template <class ST, int MODE>
+__global__ void __launch_bounds__(256, 4) aa_batch_odd(const AAParams* __restrict__ inst, const int4* __restrict__ units,
+                                                       int nunits, double* __restrict__ partials) {
+    constexpr bool STATS = MODE == 2;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int4 w = units[u];
+        const AAParams p = inst[w.x];   // the fields the unit uses, in registers
+        const int segs = (p.nx + (int)blockDim.x - 1) / (int)blockDim.x;
+        double acc[NSTAT];
+#pragma unroll
+        for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
+        for (int sg = w.y; sg < w.y + w.z; ++sg) {
+            const int row = sg / segs;
+            const int x = (sg - row * segs) * (int)blockDim.x + (int)threadIdx.x;
+            if (x < p.nx) odd_cell<ST, true, MODE, uint32_t>(p, (uint32_t)row, x, acc);
+        }
+        if constexpr (STATS) block_reduce_into(acc, partials + (size_t)u * NSTAT);
+    }
+}
+
+// out[i*NSTAT + k] = sum of partials[u*NSTAT + k] over the units u of instance i,
+// which are the contiguous range first[i] .. first[i+1]-1 (fixed order)
+__global__ void batch_finalize(const double* __restrict__ partials, const int* __restrict__ first, int n,
+                               double* __restrict__ out) {
+    const int i = blockIdx.x;
+    if (i >= n) return;
+    double acc[NSTAT];
+#pragma unroll
+    for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
+    for (int u = first[i] + threadIdx.x; u < first[i + 1]; u += blockDim.x)
+#pragma unroll
+        for (int k = 0; k < NSTAT; ++k) acc[k] += partials[(size_t)u * NSTAT + k];
+    block_reduce_into(acc, out + (size_t)i * NSTAT);
+}
+
 }  // namespace
+
+cudaError_t launch_aa_batch(const AAParams* d_inst, const int4* d_units, int nunits, int parity, int stats,
+                            int storage, int blocks, int threads, double* partials, cudaStream_t s) {
+    if (storage != 0) return cudaErrorInvalidValue;   // the batch runs FP32 populations
+    if (nunits <= 0) return cudaSuccess;
+    if (parity == 0) {
+        if (stats) aa_batch_even<StoreF32, 2><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+        else aa_batch_even<StoreF32, 0><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+    } else {
+        if (stats) aa_batch_odd<StoreF32, 2><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+        else aa_batch_odd<StoreF32, 0><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_finalize(const double* partials, const int* d_first, int n, double* out, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    batch_finalize<<<n, 256, 0, s>>>(partials, d_first, n, out);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_aa_step(const AAParams& p, int storage, int parity, LaunchCfg cfg, cudaStream_t s) {
     switch (storage) {

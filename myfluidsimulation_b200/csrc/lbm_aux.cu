@@ -49,7 +49,7 @@ __global__ void aa_reinit(typename ST::T* f, float r0, int64_t N, const float* r
 template <class T> __device__ __forceinline__ void st_mom(T* p, int k, float r0, float v);
 template <> __device__ __forceinline__ void st_mom<float>(float* p, int k, float r0, float v) { *p = v; }
 template <> __device__ __forceinline__ void st_mom<__half>(__half* p, int k, float r0, float v) {
-    *p = __float2half_rn(k == 0 ? v - r0 : v);
+    *p = __float2half_rn((k == 0 ? v - r0 : v) * kF16Scale);   // the HOME F16 layout (lbm_home.cu)
 }
 template <> __device__ __forceinline__ void st_mom<__nv_bfloat16>(__nv_bfloat16* p, int k, float r0, float v) {
     *p = __float2bfloat16_rn(k == 0 ? v - r0 : v);

@@ -566,3 +566,294 @@ int lbm_voxelize(const float* tris, int64_t ntri, const float* bb_in, const lbm_
 }
 
 }  // extern "C"
+
+// ---- batched instances -------------------------------------------------------
+struct lbm_batch {
+    std::vector<lbm_solver*> inst;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    lbm::AAParams* d_params = nullptr;
+    int4* d_units[2] = {nullptr, nullptr};
+    int* d_first[2] = {nullptr, nullptr};
+    int nunits[2] = {0, 0};
+    int units_threads = 0, units_even = 0, units_odd = 0;   // shape the unit lists were built for
+    double* partials = nullptr;
+    size_t partials_cap = 0;
+    double* d_stats = nullptr;
+    int parity = 0;
+    bool stats_on = false;
+    lbm_batch_tuning tune{256, 4, 512, 8, 0.f};
+    cudaGraphExec_t gexec = nullptr;
+    int g_sub = 0, g_parity = -1, g_stats = -1;
+};
+
+namespace {
+
+void batch_drop_graph(lbm_batch* b) {
+    if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
+    b->g_sub = 0; b->g_parity = -1; b->g_stats = -1;
+}
+
+int batch_upload_params(lbm_batch* b) {
+    for (lbm_solver* s : b->inst)
+        if (s->parity != b->inst[0]->parity) {
+            set_error("lbm_batch: instances at different step parities");
+            return LBM_ERR_INVALID;
+        }
+    b->parity = b->inst[0]->parity;
+    std::vector<lbm::AAParams> h(b->inst.size());
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        lbm_solver* s = b->inst[i];
+        h[i] = aa_params(s, false, false);
+        h[i].flags = s->flags;   // the batched kernels read the flag byte of every instance
+    }
+    CK(cudaMemcpyAsync(b->d_params, h.data(), sizeof(lbm::AAParams) * h.size(), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    batch_drop_graph(b);
+    return LBM_OK;
+}
+
+// unit lists of both parities for the current launch shape
+int batch_build_units(lbm_batch* b) {
+    const int T = b->tune.threads, E = b->tune.even_unit, O = b->tune.odd_unit;
+    if (b->units_threads == T && b->units_even == E && b->units_odd == O && b->d_units[0]) return LBM_OK;
+    for (int par = 0; par < 2; ++par) {
+        std::vector<int4> u;
+        std::vector<int> first;
+        for (size_t i = 0; i < b->inst.size(); ++i) {
+            const lbm_solver* s = b->inst[i];
+            first.push_back((int)u.size());
+            const int64_t total = par == 0 ? s->N / 2
+                                           : (int64_t)((s->dom.nx + T - 1) / T) * s->dom.ny * s->dom.nz;
+            const int step = par == 0 ? E : O;
+            for (int64_t f = 0; f < total; f += step)
+                u.push_back(make_int4((int)i, (int)f, (int)std::min<int64_t>(step, total - f), 0));
+        }
+        first.push_back((int)u.size());
+        cudaFree(b->d_units[par]);
+        cudaFree(b->d_first[par]);
+        b->d_units[par] = nullptr;
+        b->d_first[par] = nullptr;
+        CK(cudaMalloc((void**)&b->d_units[par], sizeof(int4) * std::max<size_t>(u.size(), 1)));
+        CK(cudaMalloc((void**)&b->d_first[par], sizeof(int) * first.size()));
+        CK(cudaMemcpy(b->d_units[par], u.data(), sizeof(int4) * u.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(b->d_first[par], first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+        b->nunits[par] = (int)u.size();
+    }
+    const size_t need = (size_t)std::max(b->nunits[0], b->nunits[1]) * lbm::NSTAT;
+    if (need > b->partials_cap) {
+        cudaFree(b->partials);
+        b->partials = nullptr;
+        CK(cudaMalloc((void**)&b->partials, sizeof(double) * need));
+        b->partials_cap = need;
+    }
+    b->units_threads = T; b->units_even = E; b->units_odd = O;
+    batch_drop_graph(b);
+    return LBM_OK;
+}
+
+int batch_enqueue(lbm_batch* b, int n) {
+    const int blocks_cap = lbm::num_sms() * b->tune.blocks_per_sm;
+    for (int i = 0; i < n; ++i) {
+        const bool st = b->stats_on && i == n - 1;
+        const int par = b->parity;
+        const int blocks = std::max(1, std::min(blocks_cap, b->nunits[par]));
+        CK(lbm::launch_aa_batch(b->d_params, b->d_units[par], b->nunits[par], par, st, 0, blocks, b->tune.threads,
+                                b->partials, b->stream));
+        if (st) CK(lbm::launch_batch_finalize(b->partials, b->d_first[par], (int)b->inst.size(), b->d_stats, b->stream));
+        b->parity ^= 1;
+    }
+    return LBM_OK;
+}
+
+void batch_advance_instances(lbm_batch* b, int n) {
+    for (lbm_solver* s : b->inst) {
+        s->parity ^= (n & 1);
+        s->steps += n;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_batch_create(lbm_solver* const* solvers, int32_t n, void* stream, lbm_batch** out) {
+    if (!solvers || n <= 0 || !out) { set_error("lbm_batch_create: bad argument"); return LBM_ERR_INVALID; }
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        const lbm_solver* s = solvers[i];
+        if (!s) { set_error("lbm_batch_create: null solver"); return LBM_ERR_INVALID; }
+        if (!is_aa(s) || is_ref_push(s) || s->storage != LBM_STORE_F32) {
+            set_error("lbm_batch_create: instances must be Legacy/Hybrid, FP32, halfway bounce-back");
+            return LBM_ERR_UNSUPPORTED;
+        }
+        if (s->N % 2 != 0 || (uint64_t)s->N * 19u >= (1ull << 32)) {
+            set_error("lbm_batch_create: instance cell counts must be even and below 2^32/19");
+            return LBM_ERR_SIZE;
+        }
+        if (s->parity != solvers[0]->parity) {
+            set_error("lbm_batch_create: instances at different step parities");
+            return LBM_ERR_INVALID;
+        }
+    }
+    lbm_batch* b = new lbm_batch();
+    b->inst.assign(solvers, solvers + n);
+    b->parity = solvers[0]->parity;
+    if (stream) b->stream = static_cast<cudaStream_t>(stream);
+    else {
+        if (cudaStreamCreate(&b->stream) != cudaSuccess) { delete b; set_error("lbm_batch_create: stream"); return LBM_ERR_CUDA; }
+        b->own_stream = true;
+    }
+    // the instances' own streams finish their queued work first
+    for (lbm_solver* s : b->inst)
+        if (cudaStreamSynchronize(s->stream) != cudaSuccess) { lbm_batch_destroy(b); set_error("lbm_batch_create: sync"); return LBM_ERR_CUDA; }
+    if (cudaMalloc((void**)&b->d_params, sizeof(lbm::AAParams) * n) != cudaSuccess ||
+        cudaMalloc((void**)&b->d_stats, sizeof(double) * lbm::NSTAT * n) != cudaSuccess) {
+        lbm_batch_destroy(b);
+        set_error("lbm_batch_create: allocation failed");
+        return LBM_ERR_ALLOC;
+    }
+    cudaMemset(b->d_stats, 0, sizeof(double) * lbm::NSTAT * n);
+    int rc = batch_upload_params(b);
+    if (rc == LBM_OK) rc = batch_build_units(b);
+    if (rc != LBM_OK) { lbm_batch_destroy(b); return rc; }
+    *out = b;
+    return LBM_OK;
+}
+
+int lbm_batch_refresh(lbm_batch* b) {
+    if (!b) { set_error("lbm_batch_refresh: null batch"); return LBM_ERR_INVALID; }
+    return batch_upload_params(b);
+}
+
+int lbm_batch_destroy(lbm_batch* b) {
+    if (!b) return LBM_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    cudaFree(b->d_params); cudaFree(b->d_units[0]); cudaFree(b->d_units[1]);
+    cudaFree(b->d_first[0]); cudaFree(b->d_first[1]); cudaFree(b->partials); cudaFree(b->d_stats);
+    if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return LBM_OK;
+}
+
+int lbm_batch_set_tuning(lbm_batch* b, const lbm_batch_tuning* t) {
+    if (!b || !t) { set_error("lbm_batch_set_tuning: null argument"); return LBM_ERR_INVALID; }
+    if ((t->threads != 128 && t->threads != 256) || t->blocks_per_sm < 1 || t->blocks_per_sm > 16 ||
+        t->even_unit < 1 || t->odd_unit < 1) {
+        set_error("lbm_batch_set_tuning: threads 128|256, blocks_per_sm 1..16, units >= 1");
+        return LBM_ERR_INVALID;
+    }
+    b->tune = *t;
+    return batch_build_units(b);
+}
+
+int lbm_batch_get_tuning(lbm_batch* b, lbm_batch_tuning* out) {
+    if (!b || !out) { set_error("lbm_batch_get_tuning: null argument"); return LBM_ERR_INVALID; }
+    *out = b->tune;
+    return LBM_OK;
+}
+
+int lbm_batch_tune(lbm_batch* b, int32_t trial_pairs, lbm_batch_tuning* out) {
+    if (!b) { set_error("lbm_batch_tune: null batch"); return LBM_ERR_INVALID; }
+    if (trial_pairs < 1) trial_pairs = 1;
+    const bool saved_stats = b->stats_on;
+    b->stats_on = false;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    lbm_batch_tuning best = b->tune;
+    float best_ms = 1e30f;
+    for (int threads : {128, 256})
+        for (int bps : {2, 4, 8})
+            for (int ev : {threads, 4 * threads, 16 * threads})
+                for (int od : {1, 4, 16}) {
+                    if (threads * bps > 2048) continue;
+                    lbm_batch_tuning t{threads, bps, ev, od, 0.f};
+                    b->tune = t;
+                    int rc = batch_build_units(b);
+                    if (rc != LBM_OK) return rc;
+                    rc = batch_enqueue(b, 2);              // warm-up pair
+                    if (rc != LBM_OK) return rc;
+                    CK(cudaEventRecord(e0, b->stream));
+                    rc = batch_enqueue(b, 2 * trial_pairs);
+                    if (rc != LBM_OK) return rc;
+                    CK(cudaEventRecord(e1, b->stream));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    batch_advance_instances(b, 2 + 2 * trial_pairs);
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = t;
+                        best.us_per_step = 1e3f * ms / (2 * trial_pairs);
+                    }
+                }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tune = best;
+    b->stats_on = saved_stats;
+    const int rc = batch_build_units(b);
+    if (rc != LBM_OK) return rc;
+    if (out) *out = best;
+    return LBM_OK;
+}
+
+int lbm_batch_step(lbm_batch* b, int32_t substeps) {
+    if (!b) { set_error("lbm_batch_step: null batch"); return LBM_ERR_INVALID; }
+    if (substeps < 0) { set_error("lbm_batch_step: negative substeps"); return LBM_ERR_INVALID; }
+    for (const lbm_solver* s : b->inst)
+        if (s->parity != b->parity) {
+            set_error("lbm_batch_step: an instance was stepped or reinitialised outside the batch; "
+                      "call lbm_batch_refresh");
+            return LBM_ERR_INVALID;
+        }
+    if (substeps == 0) return LBM_OK;
+    if (substeps == 1) {
+        const int rc = batch_enqueue(b, 1);
+        if (rc == LBM_OK) batch_advance_instances(b, 1);
+        return rc;
+    }
+    // multi-step calls replay a captured graph of `substeps` persistent launches
+    if (!b->gexec || b->g_sub != substeps || b->g_parity != b->parity || b->g_stats != (int)b->stats_on) {
+        batch_drop_graph(b);
+        const int saved = b->parity;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = batch_enqueue(b, substeps);
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        b->parity = saved;
+        if (rc != LBM_OK) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) { set_error(std::string("batch graph capture: ") + cudaGetErrorString(e)); return LBM_ERR_CUDA; }
+        const cudaError_t e2 = cudaGraphInstantiate(&b->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (e2 != cudaSuccess) { set_error(std::string("batch graph: ") + cudaGetErrorString(e2)); return LBM_ERR_CUDA; }
+        b->g_sub = substeps; b->g_parity = b->parity; b->g_stats = b->stats_on;
+    }
+    CK(cudaGraphLaunch(b->gexec, b->stream));
+    b->parity ^= (substeps & 1);
+    batch_advance_instances(b, substeps);
+    return LBM_OK;
+}
+
+int lbm_batch_synchronize(lbm_batch* b) {
+    if (!b) { set_error("lbm_batch_synchronize: null batch"); return LBM_ERR_INVALID; }
+    CK(cudaStreamSynchronize(b->stream));
+    return LBM_OK;
+}
+
+int lbm_batch_enable_stats(lbm_batch* b, int enable) {
+    if (!b) { set_error("lbm_batch_enable_stats: null batch"); return LBM_ERR_INVALID; }
+    b->stats_on = enable != 0;
+    return LBM_OK;
+}
+
+int lbm_batch_get_stats(lbm_batch* b, double* out) {
+    if (!b || !out) { set_error("lbm_batch_get_stats: null argument"); return LBM_ERR_INVALID; }
+    CK(cudaMemcpyAsync(out, b->d_stats, sizeof(double) * lbm::NSTAT * b->inst.size(), cudaMemcpyDeviceToHost,
+                       b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return LBM_OK;
+}
+
+}  // extern "C"

@@ -47,6 +47,47 @@ __host__ __device__ constexpr float wq(int q) {
     return q == 0 ? 1.0f / 3.0f : (q <= 6 ? 1.0f / 18.0f : 1.0f / 36.0f);
 }
 
+// Products with the lattice constants 1/3, 1/6, 1/18 and 1/36, rounded as if
+// the constant were exact: c x = fma(c_hi, x, c_lo x) with c_hi = float(c) and
+// c_lo = float(c - c_hi).  A plain product with float(c) carries the constant's
+// own rounding error into every step as a bias (float(1/6) is 3e-8 too large,
+// so momentum rebuilt with it grows by 3e-8 per step, 3e-5 after 1000 steps);
+// with the split the rounding is that of one correctly rounded product.
+constexpr float K3_HI = 0x1.555556p-2f, K3_LO = -0x1.555556p-27f;     // 1/3
+constexpr float K6_HI = 0x1.555556p-3f, K6_LO = -0x1.555556p-28f;     // 1/6
+constexpr float K18_HI = 0x1.c71c72p-5f, K18_LO = -0x1.c71c72p-32f;   // 1/18
+constexpr float K36_HI = 0x1.c71c72p-6f, K36_LO = -0x1.c71c72p-33f;   // 1/36
+__device__ __forceinline__ float mulk(float x, float hi, float lo) { return __fmaf_rn(hi, x, __fmul_rn(lo, x)); }
+__device__ __forceinline__ float2 mulk(float2 x, float hi, float lo) {
+    return __ffma2_rn(make_float2(hi, hi), x, __fmul2_rn(make_float2(lo, lo), x));
+}
+
+// ---- stochastic rounding to F16/BF16 pairs (sm_100a cvt.rs) ---------------
+// The narrow stores of a smooth field round neighbouring cells the same way,
+// so round-to-nearest errors add up coherently over the steps; rounding up or
+// down at random, with probability given by the distance to each neighbour,
+// makes every store unbiased and the errors independent.  The random bits are a
+// hash of the stored values and of a per-value salt (no state, so the step is
+// still a pure function of its input and can be replayed in a graph).
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+    x ^= x >> 16; x *= 0x7feb352du; x ^= x >> 15; x *= 0x846ca68bu; x ^= x >> 16;
+    return x;
+}
+__device__ __forceinline__ uint32_t sr_bits(float a, float b, uint32_t salt) {
+    return mix32(salt ^ __float_as_uint(a) ^ (__float_as_uint(b) * 0x9e3779b9u));
+}
+// {lo, hi} -> packed f16x2 (lo in the low half), stochastically rounded
+__device__ __forceinline__ uint32_t cvt_rs_f16x2(float lo, float hi, uint32_t rb) {
+    uint32_t d;
+    asm("cvt.rs.satfinite.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rb));
+    return d;
+}
+__device__ __forceinline__ uint32_t cvt_rs_bf16x2(float lo, float hi, uint32_t rb) {
+    uint32_t d;
+    asm("cvt.rs.satfinite.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rb));
+    return d;
+}
+
 // flag byte per cell, built on the device from the solid mask
 enum : uint8_t {
     F_SOLID = 1,     // solid cell (frozen populations, macros 1,0,0,0)
@@ -89,14 +130,19 @@ struct StoreF32 {
     }
 };
 
+// F16 keeps the shifted value scaled by 2^10 (exact in FP32): |f - w rho0| < 64
+// fits, and deviations down to 6e-8 stay normal numbers instead of subnormals.
+constexpr float kF16Scale = 1024.0f;
+constexpr float kF16Inv = 1.0f / 1024.0f;
+
 struct StoreF16 {
     using T = __half;
     static constexpr int kId = 1;
     __device__ __forceinline__ static float ld(const T* p, int q, float r0) {
-        return __half2float(*p) + wq(q) * r0;
+        return __half2float(*p) * kF16Inv + wq(q) * r0;
     }
     __device__ __forceinline__ static void st(T* p, int q, float r0, float v) {
-        *p = __float2half_rn(v - wq(q) * r0);
+        *p = __float2half_rn((v - wq(q) * r0) * kF16Scale);
     }
     __device__ __forceinline__ static void ld4(const T* p, int q, float r0, float* o) {
         const uint2 raw = *reinterpret_cast<const uint2*>(p);
@@ -104,12 +150,12 @@ struct StoreF16 {
         const __half2 b = *reinterpret_cast<const __half2*>(&raw.y);
         const float s = wq(q) * r0;
         const float2 fa = __half22float2(a), fb = __half22float2(b);
-        o[0] = fa.x + s; o[1] = fa.y + s; o[2] = fb.x + s; o[3] = fb.y + s;
+        o[0] = fa.x * kF16Inv + s; o[1] = fa.y * kF16Inv + s; o[2] = fb.x * kF16Inv + s; o[3] = fb.y * kF16Inv + s;
     }
     __device__ __forceinline__ static void st4(T* p, int q, float r0, const float* v) {
         const float s = wq(q) * r0;
-        __half2 a = __floats2half2_rn(v[0] - s, v[1] - s);
-        __half2 b = __floats2half2_rn(v[2] - s, v[3] - s);
+        __half2 a = __floats2half2_rn((v[0] - s) * kF16Scale, (v[1] - s) * kF16Scale);
+        __half2 b = __floats2half2_rn((v[2] - s) * kF16Scale, (v[3] - s) * kF16Scale);
         uint2 raw;
         raw.x = *reinterpret_cast<uint32_t*>(&a);
         raw.y = *reinterpret_cast<uint32_t*>(&b);
@@ -118,11 +164,11 @@ struct StoreF16 {
     __device__ __forceinline__ static void ld2(const T* p, int q, float r0, float* o) {
         const float2 f = __half22float2(*reinterpret_cast<const __half2*>(p));
         const float s = wq(q) * r0;
-        o[0] = f.x + s; o[1] = f.y + s;
+        o[0] = f.x * kF16Inv + s; o[1] = f.y * kF16Inv + s;
     }
     __device__ __forceinline__ static void st2(T* p, int q, float r0, const float* v) {
         const float s = wq(q) * r0;
-        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(v[0] - s, v[1] - s);
+        *reinterpret_cast<__half2*>(p) = __floats2half2_rn((v[0] - s) * kF16Scale, (v[1] - s) * kF16Scale);
     }
 };
 

@@ -14,13 +14,18 @@
 //     4.5 (c.u)^2 - 1.5 u^2 = 4.5 Q:uu), in opposite-pair form, into a shared
 //     ring grouped by c_z: the up-going group lives 3 planes, the in-plane group
 //     2 and the down-going group 1 (38 floats per position; halo positions write
-//     only the 5, or 1, populations that point into the tile);
+//     only the 5, or 1, populations that point into the tile, with the same
+//     expressions as a tile cell);
+//   * the populations are shifted, g_q = f*_q - w_q rho0 (see Coef), and every
+//     product with 1/3, 1/6 or 1/18 is rounded as if the constant were exact
+//     (mulk), so FP32 rounding adds no drift of mass, momentum or stress;
 //   * a link that does not stream (solid neighbour, duct inlet/outlet) is
 //     handled by the gathering cell, which writes the replacement into the slot
 //     of the source it would have gathered from (each slot has one reader);
-//   * the gather is 19 shared-memory loads and pair sums.
+//   * the gather is 19 shared-memory loads and pair sums;
+//   * F16/BF16 moments are stored with stochastic rounding (cvt.rs).
 // DRAM traffic is the 10 moments read once and written once (80 B per cell in
-// FP32) plus the halo re-reads that L2 does not absorb.
+// FP32, 40 B in F16/BF16) plus the halo re-reads that L2 does not absorb.
 #include "lbm_common.cuh"
 #include "lbm_internal.h"
 
@@ -52,7 +57,7 @@ struct Ring {
     float* mid;
     float* dn;
     __device__ __forceinline__ Ring(float* sm, int p) {
-        up = sm + (((p % 3) + 3) % 3) * UP_SZ;
+        up = sm + (p < 0 ? p + 3 : p % 3) * UP_SZ;   // p >= -1
         mid = sm + MID_OFF + (p & 1) * MID_SZ;
         dn = sm + DN_OFF;
     }
@@ -62,72 +67,83 @@ struct Ring {
     }
 };
 
-// Moment storage: F32 as is; F16/BF16 keep rho - rho0, u and S.
-template <class T> struct MomStore;
-template <> struct MomStore<float> {
-    __device__ __forceinline__ static float ld(const float* p, int k, float r0) { return __ldg(p); }
-    __device__ __forceinline__ static void st(float* p, int k, float r0, float v) { *p = v; }
-};
-template <> struct MomStore<__half> {
-    __device__ __forceinline__ static float ld(const __half* p, int k, float r0) {
-        return __half2float(*p) + (k == 0 ? r0 : 0.f);
-    }
-    __device__ __forceinline__ static void st(__half* p, int k, float r0, float v) {
-        *p = __float2half_rn(k == 0 ? v - r0 : v);
-    }
-};
-template <> struct MomStore<__nv_bfloat16> {
-    __device__ __forceinline__ static float ld(const __nv_bfloat16* p, int k, float r0) {
-        return __bfloat162float(*p) + (k == 0 ? r0 : 0.f);
-    }
-    __device__ __forceinline__ static void st(__nv_bfloat16* p, int k, float r0, float v) {
-        *p = __float2bfloat16_rn(k == 0 ? v - r0 : v);
+// ---- scalar and paired FP32 arithmetic with identical rounding -------------
+__device__ __forceinline__ float vadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float vsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float vmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float vsplat(float s, float) { return s; }
+__device__ __forceinline__ float2 vadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 vsub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 vmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 vfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 vsplat(float s, float2) { return make_float2(s, s); }
+
+// Rebuild coefficients of one cell (V = float) or two (V = float2), pre-scaled
+// by w1 = 1/18 (w0 = 6 w1, w2 = w1/2):
+//   P = w1 (rho - rho0 - 1.5 tr B),  a_k = 3 w1 rho u_k,  b_kk = 4.5 w1 B_kk,
+//   b_kl = 9 w1 B_kl,  B = rho u u + (1 - w) S.
+// The populations built from them are SHIFTED, g_q = f*_q - w_q rho0: the
+// moments gathered from g carry the small deviations from the rest state
+// instead of the O(1) constant part (sum g = rho - rho0, sum c c g = Pi -
+// rho0/3 I), which keeps the FP32 cancellation in S = Pi - rho/3 I - rho u u
+// at the size of the deviations.
+template <class V>
+struct Coef {
+    V P, ax, ay, az, bxx, byy, bzz, bxy, bxz, byz;
+    __device__ __forceinline__ void set(const V (&m)[10], float omw_s, float r0) {
+        const V omw = vsplat(omw_s, V{});
+        const V r = m[0];
+        const V jx = vmul(r, m[1]), jy = vmul(r, m[2]), jz = vmul(r, m[3]);
+        const V Bxx = vfma(jx, m[1], vmul(omw, m[4]));
+        const V Bxy = vfma(jx, m[2], vmul(omw, m[5]));
+        const V Bxz = vfma(jx, m[3], vmul(omw, m[6]));
+        const V Byy = vfma(jy, m[2], vmul(omw, m[7]));
+        const V Byz = vfma(jy, m[3], vmul(omw, m[8]));
+        const V Bzz = vfma(jz, m[3], vmul(omw, m[9]));
+        constexpr float w1 = 1.0f / 18.0f;
+        P = mulk(vfma(vsplat(-1.5f, V{}), vadd(vadd(Bxx, Byy), Bzz), vsub(r, vsplat(r0, V{}))), K18_HI, K18_LO);
+        const V b45 = vsplat(4.5f * w1, V{}), b9 = vsplat(9.0f * w1, V{});   // 1/4 and 1/2, exact
+        ax = mulk(jx, K6_HI, K6_LO); ay = mulk(jy, K6_HI, K6_LO); az = mulk(jz, K6_HI, K6_LO);
+        bxx = vmul(b45, Bxx); byy = vmul(b45, Byy); bzz = vmul(b45, Bzz);
+        bxy = vmul(b9, Bxy); bxz = vmul(b9, Bxz); byz = vmul(b9, Byz);
     }
 };
 
-// Rebuild coefficients of one cell, pre-scaled by w1 = 1/18 (w0 = 6 w1, w2 = w1/2):
-//   P = w1 (rho - 1.5 tr B),  a_k = 3 w1 rho u_k,  b_kk = 4.5 w1 B_kk,  b_kl = 9 w1 B_kl,
-//   B = rho u u + (1 - w) S.  Then f*_q = P + sum_k c_k a_k + sum_k c_k^2 b_kk
-//   + sum_{k<l} c_k c_l b_kl for the axis directions, half of that for the
-//   diagonals, and 6 P for the rest direction.
-struct Coef {
-    float P, ax, ay, az, bxx, byy, bzz, bxy, bxz, byz;
-    __device__ __forceinline__ void set(const float (&m)[10], float omw) {
-        const float r = m[0];
-        const float jx = r * m[1], jy = r * m[2], jz = r * m[3];
-        const float Bxx = fmaf(jx, m[1], omw * m[4]);
-        const float Bxy = fmaf(jx, m[2], omw * m[5]);
-        const float Bxz = fmaf(jx, m[3], omw * m[6]);
-        const float Byy = fmaf(jy, m[2], omw * m[7]);
-        const float Byz = fmaf(jy, m[3], omw * m[8]);
-        const float Bzz = fmaf(jz, m[3], omw * m[9]);
-        constexpr float w1 = 1.0f / 18.0f;
-        P = w1 * fmaf(-1.5f, Bxx + Byy + Bzz, r);
-        ax = (3.0f * w1) * jx; ay = (3.0f * w1) * jy; az = (3.0f * w1) * jz;
-        bxx = (4.5f * w1) * Bxx; byy = (4.5f * w1) * Byy; bzz = (4.5f * w1) * Bzz;
-        bxy = (9.0f * w1) * Bxy; bxz = (9.0f * w1) * Bxz; byz = (9.0f * w1) * Byz;
-    }
-    // one population (halo positions and the boundary path)
-    template <int q>
-    __device__ __forceinline__ float fpost() const {
+// Post-collision population q from the coefficients: the same expression for
+// every position and role (tile cell, halo, bounce-back), in opposite-pair form.
+template <int q, class V>
+__device__ __forceinline__ V fpost(const Coef<V>& c) {
+    const V half = vsplat(0.5f, V{});
+    if constexpr (q == 0) {
+        return vmul(vsplat(6.0f, V{}), c.P);
+    } else if constexpr (q <= 6) {
+        constexpr int k = (q - 1) / 2;               // axis
+        constexpr bool plus = (q & 1) == 1;
+        const V b = vadd(c.P, k == 0 ? c.bxx : (k == 1 ? c.byy : c.bzz));
+        const V a = k == 0 ? c.ax : (k == 1 ? c.ay : c.az);
+        return plus ? vadd(b, a) : vsub(b, a);
+    } else {
+        // diagonal in the plane of axes (i, j), i < j; sign s of the second component
         constexpr int X = cx(q), Y = cy(q), Z = cz(q);
-        if constexpr (q == 0) {
-            return 6.0f * P;
+        constexpr int i = X != 0 ? 0 : 1;
+        constexpr int j = Z != 0 ? 2 : 1;
+        constexpr int si = i == 0 ? X : Y;
+        constexpr int sj = j == 1 ? Y : Z;
+        const V bi = vadd(c.P, i == 0 ? c.bxx : c.byy);          // P + b_ii
+        const V b = vadd(bi, j == 1 ? c.byy : c.bzz);             // + b_jj
+        const V bij = (i == 0 && j == 1) ? c.bxy : ((i == 0) ? c.bxz : c.byz);
+        const V ai = i == 0 ? c.ax : c.ay;
+        const V aj = j == 1 ? c.ay : c.az;
+        if constexpr (si * sj > 0) {
+            const V bp = vadd(b, bij), sp = vadd(ai, aj);
+            return vmul(half, si > 0 ? vadd(bp, sp) : vsub(bp, sp));
         } else {
-            float s = P;
-            if (X) s += X > 0 ? ax : -ax;
-            if (Y) s += Y > 0 ? ay : -ay;
-            if (Z) s += Z > 0 ? az : -az;
-            if (X) s += bxx;
-            if (Y) s += byy;
-            if (Z) s += bzz;
-            if (X && Y) s += X * Y > 0 ? bxy : -bxy;
-            if (X && Z) s += X * Z > 0 ? bxz : -bxz;
-            if (Y && Z) s += Y * Z > 0 ? byz : -byz;
-            return ((X != 0) + (Y != 0) + (Z != 0)) == 2 ? 0.5f * s : s;
+            const V bm = vsub(b, bij), sn = vsub(ai, aj);
+            return vmul(half, si > 0 ? vadd(bm, sn) : vsub(bm, sn));
         }
     }
-};
+}
 
 template <int q> struct QI { static constexpr int value = q; };
 template <int Q0, int Q1, class F>
@@ -138,77 +154,90 @@ __device__ __forceinline__ void static_for(F&& fn) {
     }
 }
 
-// A tile cell writes all 19 populations leaving its plane.
-__device__ __forceinline__ void build_tile_cell(const Ring& R, int pos, const Coef& c) {
-    R.at<0>(pos) = 6.0f * c.P;
-    const float bx = c.P + c.bxx, by = c.P + c.byy, bz = c.P + c.bzz;
-    R.at<1>(pos) = bx + c.ax;
-    R.at<2>(pos) = bx - c.ax;
-    R.at<3>(pos) = by + c.ay;
-    R.at<4>(pos) = by - c.ay;
-    R.at<5>(pos) = bz + c.az;
-    R.at<6>(pos) = bz - c.az;
-    {
-        const float b = bx + c.byy, bp = b + c.bxy, bm = b - c.bxy;
-        const float sp = c.ax + c.ay, sn = c.ax - c.ay;
-        R.at<7>(pos) = 0.5f * (bp + sp);     // (+1,+1,0)
-        R.at<10>(pos) = 0.5f * (bp - sp);    // (-1,-1,0)
-        R.at<9>(pos) = 0.5f * (bm + sn);     // (+1,-1,0)
-        R.at<8>(pos) = 0.5f * (bm - sn);     // (-1,+1,0)
+// ---- moment storage: F32 as is; F16/BF16 keep rho - rho0, u and S ---------
+template <class T> struct MomStore;
+template <> struct MomStore<float> {
+    __device__ __forceinline__ static float ld(const float* p, int k, float r0) { return __ldg(p); }
+    __device__ __forceinline__ static float2 ld2(const float* p, int k, float r0) {
+        return __ldg(reinterpret_cast<const float2*>(p));
     }
-    {
-        const float b = bx + c.bzz, bp = b + c.bxz, bm = b - c.bxz;
-        const float sp = c.ax + c.az, sn = c.ax - c.az;
-        R.at<11>(pos) = 0.5f * (bp + sp);    // (+1,0,+1)
-        R.at<14>(pos) = 0.5f * (bp - sp);    // (-1,0,-1)
-        R.at<13>(pos) = 0.5f * (bm + sn);    // (+1,0,-1)
-        R.at<12>(pos) = 0.5f * (bm - sn);    // (-1,0,+1)
+    __device__ __forceinline__ static void st(float* p, int k, float r0, float v, uint32_t) { *p = v; }
+    __device__ __forceinline__ static void st2(float* p, int k, float r0, float2 v, uint32_t) {
+        *reinterpret_cast<float2*>(p) = v;
     }
-    {
-        const float b = by + c.bzz, bp = b + c.byz, bm = b - c.byz;
-        const float sp = c.ay + c.az, sn = c.ay - c.az;
-        R.at<15>(pos) = 0.5f * (bp + sp);    // (0,+1,+1)
-        R.at<18>(pos) = 0.5f * (bp - sp);    // (0,-1,-1)
-        R.at<17>(pos) = 0.5f * (bm + sn);    // (0,+1,-1)
-        R.at<16>(pos) = 0.5f * (bm - sn);    // (0,-1,+1)
+};
+// F16: (rho - rho0, u, S) scaled by 2^10 (exact), as the F16 populations are
+template <> struct MomStore<__half> {
+    __device__ __forceinline__ static float ld(const __half* p, int k, float r0) {
+        return __half2float(*p) * kF16Inv + (k == 0 ? r0 : 0.f);
     }
-}
+    __device__ __forceinline__ static float2 ld2(const __half* p, int k, float r0) {
+        const float2 v = __half22float2(*reinterpret_cast<const __half2*>(p));
+        const float s = k == 0 ? r0 : 0.f;
+        return make_float2(v.x * kF16Inv + s, v.y * kF16Inv + s);
+    }
+    // stochastically rounded (see cvt_rs_f16x2); salt: a per-value index
+    __device__ __forceinline__ static void st(__half* p, int k, float r0, float v, uint32_t salt) {
+        const float a = (k == 0 ? v - r0 : v) * kF16Scale;
+        const uint32_t d = cvt_rs_f16x2(a, 0.f, sr_bits(a, 0.f, salt));
+        *reinterpret_cast<uint16_t*>(p) = (uint16_t)(d & 0xffffu);
+    }
+    __device__ __forceinline__ static void st2(__half* p, int k, float r0, float2 v, uint32_t salt) {
+        const float s = k == 0 ? r0 : 0.f;
+        const float a = (v.x - s) * kF16Scale, b = (v.y - s) * kF16Scale;
+        *reinterpret_cast<uint32_t*>(p) = cvt_rs_f16x2(a, b, sr_bits(a, b, salt));
+    }
+};
+template <> struct MomStore<__nv_bfloat16> {
+    __device__ __forceinline__ static float ld(const __nv_bfloat16* p, int k, float r0) {
+        return __bfloat162float(*p) + (k == 0 ? r0 : 0.f);
+    }
+    __device__ __forceinline__ static float2 ld2(const __nv_bfloat16* p, int k, float r0) {
+        const float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+        const float s = k == 0 ? r0 : 0.f;
+        return make_float2(v.x + s, v.y + s);
+    }
+    __device__ __forceinline__ static void st(__nv_bfloat16* p, int k, float r0, float v, uint32_t salt) {
+        const float a = k == 0 ? v - r0 : v;
+        const uint32_t d = cvt_rs_bf16x2(a, 0.f, sr_bits(a, 0.f, salt));
+        *reinterpret_cast<uint16_t*>(p) = (uint16_t)(d & 0xffffu);
+    }
+    __device__ __forceinline__ static void st2(__nv_bfloat16* p, int k, float r0, float2 v, uint32_t salt) {
+        const float s = k == 0 ? r0 : 0.f;
+        const float a = v.x - s, b = v.y - s;
+        *reinterpret_cast<uint32_t*>(p) = cvt_rs_bf16x2(a, b, sr_bits(a, b, salt));
+    }
+};
 
-// A halo position writes only the directions that point into the tile:
-// dir 0 = x-1 column (+x), 1 = x+TX column (-x), 2 = y-1 row (+y),
-// 3 = y+TY row (-y), 4..7 = corners feeding 7, 8, 9, 10.
-__device__ __forceinline__ void build_halo(const Ring& R, int pos, int dir, const Coef& c) {
+// A tile cell writes all 19 populations leaving its plane; a halo position
+// writes only the directions that point into the tile: dir 0 = x-1 column
+// (+x), 1 = x+TX column (-x), 2 = y-1 row (+y), 3 = y+TY row (-y), 4..7 =
+// corners feeding 7, 8, 9, 10.  The same expression (fpost) for every role.
+__device__ __forceinline__ void build(const Ring& R, int pos, int dir, const Coef<float>& c) {
+    auto put = [&](auto qi) {
+        constexpr int q = decltype(qi)::value;
+        R.template at<q>(pos) = fpost<q>(c);
+    };
     switch (dir) {
-        case 0:
-            R.at<1>(pos) = c.fpost<1>(); R.at<7>(pos) = c.fpost<7>(); R.at<9>(pos) = c.fpost<9>();
-            R.at<11>(pos) = c.fpost<11>(); R.at<13>(pos) = c.fpost<13>();
-            break;
-        case 1:
-            R.at<2>(pos) = c.fpost<2>(); R.at<8>(pos) = c.fpost<8>(); R.at<10>(pos) = c.fpost<10>();
-            R.at<12>(pos) = c.fpost<12>(); R.at<14>(pos) = c.fpost<14>();
-            break;
-        case 2:
-            R.at<3>(pos) = c.fpost<3>(); R.at<7>(pos) = c.fpost<7>(); R.at<8>(pos) = c.fpost<8>();
-            R.at<15>(pos) = c.fpost<15>(); R.at<17>(pos) = c.fpost<17>();
-            break;
-        case 3:
-            R.at<4>(pos) = c.fpost<4>(); R.at<9>(pos) = c.fpost<9>(); R.at<10>(pos) = c.fpost<10>();
-            R.at<16>(pos) = c.fpost<16>(); R.at<18>(pos) = c.fpost<18>();
-            break;
-        case 4: R.at<7>(pos) = c.fpost<7>(); break;
-        case 5: R.at<8>(pos) = c.fpost<8>(); break;
-        case 6: R.at<9>(pos) = c.fpost<9>(); break;
-        case 7: R.at<10>(pos) = c.fpost<10>(); break;
+        case -1: static_for<0, 19>(put); break;
+        case 0: put(QI<1>{}); put(QI<7>{}); put(QI<9>{}); put(QI<11>{}); put(QI<13>{}); break;
+        case 1: put(QI<2>{}); put(QI<8>{}); put(QI<10>{}); put(QI<12>{}); put(QI<14>{}); break;
+        case 2: put(QI<3>{}); put(QI<7>{}); put(QI<8>{}); put(QI<15>{}); put(QI<17>{}); break;
+        case 3: put(QI<4>{}); put(QI<9>{}); put(QI<10>{}); put(QI<16>{}); put(QI<18>{}); break;
+        case 4: put(QI<7>{}); break;
+        case 5: put(QI<8>{}); break;
+        case 6: put(QI<9>{}); break;
+        case 7: put(QI<10>{}); break;
         default: break;
     }
 }
 
-template <class T, bool STATS>
+template <class T, bool STATS, class IDX>
 __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
     extern __shared__ float sm[];
     const T* __restrict__ m = static_cast<const T*>(p.m);
     T* __restrict__ mn = static_cast<T*>(p.mn);
-    const int64_t N = p.N;
+    const IDX N = (IDX)p.N;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const float omw = 1.f - p.omega;
     const float r0 = p.rho0;
@@ -242,8 +271,8 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
     if (p.duct) exists = exists && lx >= 0 && lx < nx;
     else gx = ((lx % nx) + nx) % nx;
     const bool owner = dir == -1 && lx < nx && ly < ny;   // gathers and stores a cell
-    const int64_t plane = (int64_t)nx * ny;
-    const int64_t coff = (int64_t)gy * nx + gx;
+    const IDX plane = (IDX)nx * (IDX)ny;
+    const IDX coff = (IDX)gy * (IDX)nx + (IDX)gx;
 
     const uint8_t* __restrict__ flags = p.flags;
     float mreg[10];
@@ -253,24 +282,18 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
     auto load = [&](int z) {
         if (!exists) return;
         const int zz = z < 0 ? z + nz : (z >= nz ? z - nz : z);
-        const int64_t id = (int64_t)zz * plane + coff;
-        const T* ptr = m + id;
+        const IDX id = (IDX)zz * plane + coff;
 #pragma unroll
-        for (int c = 0; c < 10; ++c) {
-            mreg[c] = MomStore<T>::ld(ptr, c, r0);
-            ptr += N;
-        }
+        for (int c = 0; c < 10; ++c) mreg[c] = MomStore<T>::ld(m + (IDX)c * N + id, c, r0);
         freg = flags ? flags[id] : 0u;
     };
     // the moments of plane pz are in mreg/freg: write the populations leaving it
     // (a solid cell writes none; its slots are filled by its fluid neighbours)
     auto arrive = [&](int pz) {
         if (exists && !(freg & F_SOLID)) {
-            Coef c;
-            c.set(mreg, omw);
-            const Ring R(sm, pz);
-            if (dir == -1) build_tile_cell(R, pos, c);
-            else build_halo(R, pos, dir, c);
+            Coef<float> c;
+            c.set(mreg, omw, r0);
+            build(Ring(sm, pz), pos, dir, c);
         }
     };
 
@@ -293,16 +316,13 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
         // 2. a link that does not stream: the cell writes the replacement into the
         //    slot of the source it would have gathered from (read by nobody else)
         if (owner && (fcur & F_SPECIAL)) {
-            const int64_t id = (int64_t)z * plane + coff;
+            const IDX id = (IDX)z * plane + coff;
             const uint32_t lk = p.links[id];
             float own[10];
-            {
-                const T* ptr = m + id;
 #pragma unroll
-                for (int c = 0; c < 10; ++c) { own[c] = MomStore<T>::ld(ptr, c, r0); ptr += N; }
-            }
-            Coef oc;
-            oc.set(own, omw);
+            for (int c = 0; c < 10; ++c) own[c] = MomStore<T>::ld(m + (IDX)c * N + id, c, r0);
+            Coef<float> oc;
+            oc.set(own, omw, r0);
             const Ring Rm(sm, z - 1), Rz(sm, z), Rp(sm, z + 1);
             static_for<1, 19>([&](auto qi) {
                 constexpr int q = decltype(qi)::value;
@@ -310,23 +330,24 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
                     const int xs = gx - cx(q);
                     float v;
                     if (p.duct && xs < 0) {
-                        v = feq_ref(q, own[0], p.u_in, 0.f, 0.f);                      // inlet
+                        v = feq_ref(q, own[0], p.u_in, 0.f, 0.f) - wq(q) * r0;         // inlet
                     } else if (p.duct && xs >= nx) {
-                        v = oc.template fpost<q>();                                       // outlet
+                        v = fpost<q>(oc);                                                 // outlet
                     } else {
                         // own post-collision population of direction bq comes back as q
                         // (home.cu:219-225); bq = opp(q), or the reference's table
                         constexpr int bt = opp(q), br = opp_tab(q);
-                        v = p.ref_bounce ? oc.template fpost<br>() : oc.template fpost<bt>();
+                        v = p.ref_bounce ? fpost<br>(oc) : fpost<bt>(oc);
                         if (STATS) {
                             const int bq = p.ref_bounce ? br : bt;
                             const int ys = ((gy - cy(q)) % ny + ny) % ny;
                             const int zs = ((z - cz(q)) % nz + nz) % nz;
                             const int xw = ((xs % nx) + nx) % nx;
-                            if (flags[(int64_t)zs * plane + (int64_t)ys * nx + xw] & F_OBST) {
-                                acc[2] += (double)(cx(bq) - cx(q)) * (double)v;
-                                acc[3] += (double)(cy(bq) - cy(q)) * (double)v;
-                                acc[4] += (double)(cz(bq) - cz(q)) * (double)v;
+                            if (flags[(IDX)zs * plane + (IDX)ys * (IDX)nx + (IDX)xw] & F_OBST) {
+                                const double fv = (double)v + (double)(wq(q) * r0);   // unshifted
+                                acc[2] += (double)(cx(bq) - cx(q)) * fv;
+                                acc[3] += (double)(cy(bq) - cy(q)) * fv;
+                                acc[4] += (double)(cz(bq) - cz(q)) * fv;
                             }
                         }
                     }
@@ -339,12 +360,12 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
         __syncthreads();
         // 3. gather and moments
         if (owner) {
-            const int64_t id = (int64_t)z * plane + coff;
+            const IDX id = (IDX)z * plane + coff;
             T* op = mn + id;
             if (fcur & F_SOLID) {
-                MomStore<T>::st(op, 0, r0, 1.f);
 #pragma unroll
-                for (int c = 1; c < 10; ++c) MomStore<T>::st(op + c * N, c, r0, 0.f);
+                for (int c = 0; c < 10; ++c)
+                    MomStore<T>::st(op + (IDX)c * N, c, r0, c == 0 ? 1.f : 0.f, (uint32_t)id * 10u + c);
             } else {
                 const Ring Rm(sm, z - 1), Rz(sm, z), Rp(sm, z + 1);
                 float fq[19];
@@ -353,7 +374,8 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
                     const Ring& R = cz(q) > 0 ? Rm : (cz(q) == 0 ? Rz : Rp);
                     fq[q] = R.template at<q>(pos - cx(q) - HX * cy(q));
                 });
-                // moments of the gathered populations (home.cu:238-273), opposite pairs first
+                // moments of the gathered (shifted) populations (home.cu:238-273):
+                // dr = rho - rho0 = sum g, M = sum c c g = Pi - rho0/3 I; opposite pairs first
                 const float s1 = fq[1] + fq[2], d1 = fq[1] - fq[2];
                 const float s3 = fq[3] + fq[4], d3 = fq[3] - fq[4];
                 const float s5 = fq[5] + fq[6], d5 = fq[5] - fq[6];
@@ -363,7 +385,7 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
                 const float s13 = fq[13] + fq[12], d13 = fq[13] - fq[12]; // (+1,0,-1)
                 const float s15 = fq[15] + fq[18], d15 = fq[15] - fq[18]; // (0,+1,+1)
                 const float s17 = fq[17] + fq[16], d17 = fq[17] - fq[16]; // (0,+1,-1)
-                const float r = fq[0] + ((s1 + s3) + (s5 + s7)) + ((s9 + s11) + (s13 + s15) + s17);
+                const float dr = fq[0] + ((s1 + s3) + (s5 + s7)) + ((s9 + s11) + (s13 + s15) + s17);
                 const float jx = (d1 + d7) + (d9 + d11) + d13;
                 const float jy = (d3 + d7) - d9 + (d15 + d17);
                 const float jz = (d5 + d11) - d13 + (d15 - d17);
@@ -371,18 +393,16 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
                 const float Myy = (s3 + s7) + (s9 + s15) + s17;
                 const float Mzz = (s5 + s11) + (s13 + s15) + s17;
                 const float Mxy = s7 - s9, Mxz = s11 - s13, Myz = s15 - s17;
+                const float r = dr + r0;
                 const float inv = r > 0.f ? 1.0f / r : 0.f;
-                const float ux = jx * inv + p.fx, uy = jy * inv + p.fy, uz = jz * inv + p.fz;
-                const float r3 = r * (1.0f / 3.0f);
+                const float ux = fmaf(jx, inv, p.fx), uy = fmaf(jy, inv, p.fy), uz = fmaf(jz, inv, p.fz);
+                const float r3 = mulk(dr, K3_HI, K3_LO);
                 const float rx = r * ux, ry = r * uy, rz = r * uz;
                 const float out[10] = {r, ux, uy, uz,
                                        Mxx - fmaf(rx, ux, r3), Mxy - rx * uy, Mxz - rx * uz,
                                        Myy - fmaf(ry, uy, r3), Myz - ry * uz, Mzz - fmaf(rz, uz, r3)};
 #pragma unroll
-                for (int c = 0; c < 10; ++c) {
-                    MomStore<T>::st(op, c, r0, out[c]);
-                    op += N;
-                }
+                for (int c = 0; c < 10; ++c) MomStore<T>::st(op + (IDX)c * N, c, r0, out[c], (uint32_t)id * 10u + c);
                 if (STATS) {
                     acc[0] += (double)r;
                     acc[1] += 0.5 * ((double)ux * ux + (double)uy * uy + (double)uz * uz);
@@ -416,13 +436,19 @@ __global__ void home_macros(const T* __restrict__ m, int64_t N, float r0, float*
     }
 }
 
+template <class T, bool STATS>
+void launch_step(const HomeParams& p, cudaStream_t s) {
+    const int grid = home_num_blocks(p.nx, p.ny, p.nz, p.zchunk);
+    const size_t smem = sizeof(float) * SMEM_FLOATS;
+    // 32-bit element offsets while every index 10*N fits in them
+    if ((uint64_t)p.N * 10u < (1ull << 32)) home_step<T, STATS, uint32_t><<<grid, NT, smem, s>>>(p);
+    else home_step<T, STATS, int64_t><<<grid, NT, smem, s>>>(p);
+}
+
 template <class T>
 cudaError_t launch_home_t(const HomeParams& p, cudaStream_t s) {
-    const int tiles = ((p.nx + TX - 1) / TX) * ((p.ny + TY - 1) / TY);
-    const int chunks = (p.nz + p.zchunk - 1) / p.zchunk;
-    const size_t smem = sizeof(float) * SMEM_FLOATS;
-    if (p.stats) home_step<T, true><<<tiles * chunks, NT, smem, s>>>(p);
-    else home_step<T, false><<<tiles * chunks, NT, smem, s>>>(p);
+    if (p.stats) launch_step<T, true>(p, s);
+    else launch_step<T, false>(p, s);
     return cudaGetLastError();
 }
 
@@ -434,12 +460,18 @@ cudaError_t home_prepare() {
     auto set = [&](const void* fn) {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     };
-    set((const void*)home_step<float, false>);
-    set((const void*)home_step<float, true>);
-    set((const void*)home_step<__half, false>);
-    set((const void*)home_step<__half, true>);
-    set((const void*)home_step<__nv_bfloat16, false>);
-    set((const void*)home_step<__nv_bfloat16, true>);
+    set((const void*)home_step<float, false, uint32_t>);
+    set((const void*)home_step<float, true, uint32_t>);
+    set((const void*)home_step<__half, false, uint32_t>);
+    set((const void*)home_step<__half, true, uint32_t>);
+    set((const void*)home_step<__nv_bfloat16, false, uint32_t>);
+    set((const void*)home_step<__nv_bfloat16, true, uint32_t>);
+    set((const void*)home_step<float, false, int64_t>);
+    set((const void*)home_step<float, true, int64_t>);
+    set((const void*)home_step<__half, false, int64_t>);
+    set((const void*)home_step<__half, true, int64_t>);
+    set((const void*)home_step<__nv_bfloat16, false, int64_t>);
+    set((const void*)home_step<__nv_bfloat16, true, int64_t>);
     return e;
 }
 

@@ -57,6 +57,14 @@ struct LaunchCfg {
 // AA steps.  parity 0: natural layout in (the even, purely local step);
 // parity 1: the odd step (gathers from and scatters to neighbours).
 cudaError_t launch_aa_step(const AAParams& p, int storage, int parity, LaunchCfg cfg, cudaStream_t s);
+// One step of many instances in one persistent launch (FP32 populations, the
+// instances' flag bytes required); units: {instance, first, count, -} with
+// first/count in two-cell vectors (parity 0) or row segments of `threads`
+// cells (parity 1).  stats != 0 writes NSTAT sums per unit into partials.
+cudaError_t launch_aa_batch(const AAParams* d_inst, const int4* d_units, int nunits, int parity, int stats,
+                            int storage, int blocks, int threads, double* partials, cudaStream_t s);
+// per-instance sums of the unit partials: units of instance i are first[i]..first[i+1]-1
+cudaError_t launch_batch_finalize(const double* partials, const int* d_first, int n, double* out, cudaStream_t s);
 // Reference-compatible Legacy/Hybrid step (two buffers, the reference's
 // opposite table): fa -> fb.
 cudaError_t launch_ref_push(const AAParams& p, const float* fa, float* fb, LaunchCfg cfg, cudaStream_t s);

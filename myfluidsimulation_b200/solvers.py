@@ -258,3 +258,62 @@ class LBM3D_Hybrid(_RefSolver):
 __all__ = ["Domain", "Solver", "LBM3D_Legacy", "LBM3D_Home", "LBM3D_Hybrid", "METHOD_LEGACY", "METHOD_HOME",
            "METHOD_HYBRID", "STORE_F32", "STORE_F16", "STORE_BF16", "BC_PERIODIC", "BC_DUCT", "BOUNCE_HALFWAY",
            "BOUNCE_REFERENCE"]
+
+
+class Batch:
+    """Many Legacy/Hybrid solvers advanced together by one persistent launch per
+    substep (lbm_batch_* in include/lbm_capi.h).  The solvers stay owned by the
+    caller and must outlive the batch."""
+
+    def __init__(self, solvers, stream=None):
+        L = lib()
+        self._solvers = list(solvers)
+        arr = (C.c_void_p * len(self._solvers))(*[s._h.value for s in self._solvers])
+        h = C.c_void_p()
+        check(L.lbm_batch_create(arr, len(self._solvers), None if stream is None else C.c_void_p(int(stream)),
+                                 C.byref(h)))
+        self._h = h
+        self.n = len(self._solvers)
+        self.cells = sum(s.N for s in self._solvers)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def refresh(self):
+        check(lib().lbm_batch_refresh(self._h))
+
+    def tune(self, trial_pairs: int = 2) -> dict:
+        t = _lib.BatchTuning()
+        check(lib().lbm_batch_tune(self._h, int(trial_pairs), C.byref(t)))
+        return {k: getattr(t, k) for k, _ in _lib.BatchTuning._fields_}
+
+    def set_tuning(self, threads=256, blocks_per_sm=4, even_unit=512, odd_unit=8):
+        t = _lib.BatchTuning(threads, blocks_per_sm, even_unit, odd_unit, 0.0)
+        check(lib().lbm_batch_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = _lib.BatchTuning()
+        check(lib().lbm_batch_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in _lib.BatchTuning._fields_}
+
+    def step(self, n: int = 1):
+        check(lib().lbm_batch_step(self._h, int(n)))
+
+    def synchronize(self):
+        check(lib().lbm_batch_synchronize(self._h))
+
+    def enable_stats(self, on=True):
+        check(lib().lbm_batch_enable_stats(self._h, 1 if on else 0))
+
+    def stats(self) -> np.ndarray:
+        out = np.zeros((self.n, NSTAT), np.float64)
+        check(lib().lbm_batch_get_stats(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out

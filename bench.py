@@ -461,6 +461,66 @@ def batch_study(args, torch):
                       "b0": [sp["b0"] for sp in specs], "dims": [sp["dims"] for sp in specs]}))
 
 
+def adjoint_study(args, torch):
+    """The adjoint case: BGK duct 128x64x64, tau 0.6, sphere r=10 at (32,32,32);
+    controls = inlet profile u_x(y,z) = 0.04 + 0.005 N(0,1) smoothed by a 5x5 box
+    filter and the initial velocity (0.04 + 1e-3 N(0,1) in x, 1e-3 N(0,1) in y, z);
+    objective = mean drag over steps 400-500; checkpoints every 50 steps.  Times
+    the FP32 and FP64 forward+adjoint and checks the gradient against central
+    differences of the FP64 objective (eps 1e-3) on random unit directions."""
+    from myfluidsimulation_b200 import workloads as W
+    from myfluidsimulation_b200.adjoint import DuctProblem, objective
+    nx, ny, nz = 128, 64, 64
+    z, y, x = np.meshgrid(np.arange(nz) + 0.5, np.arange(ny) + 0.5, np.arange(nx) + 0.5, indexing="ij")
+    ball = ((x - 32) ** 2 + (y - 32) ** 2 + (z - 32) ** 2 <= 100).astype(np.uint8)
+    mask = W.duct_mask(nx, ny, nz, ball)
+    gen = torch.Generator().manual_seed(4)
+    raw = (0.04 + 0.005 * torch.randn((nz + 4, ny + 4), generator=gen, dtype=torch.float64)).numpy()
+    k = np.ones(5) / 5
+    ui = np.apply_along_axis(lambda r: np.convolve(r, k, "valid"), 1, raw)
+    ui = np.apply_along_axis(lambda c: np.convolve(c, k, "valid"), 0, ui)
+    u0 = 1e-3 * torch.randn((3, nz, ny, nx), generator=gen, dtype=torch.float64).numpy()
+    u0[0] += 0.04
+    prob = DuctProblem(nx, ny, nz, 0.6, mask, n_steps=500, window=(400, 500), checkpoint_every=50)
+    out = {"study": "adjoint", "workload": "duct 128x64x64, sphere r=10 at (32,32,32), tau 0.6, 500 steps, "
+                                           "J = mean drag over steps 400-500, checkpoints every 50"}
+    for prec in ("f32", "f64"):
+        objective(prob, ui, u0, prec, grad=True)          # warm-up
+        t0 = time.perf_counter()
+        J, gi, gu = objective(prob, ui, u0, prec, grad=True)
+        dt = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        objective(prob, ui, u0, prec)
+        dtf = time.perf_counter() - t0
+        out[prec] = {"J": J, "seconds_forward_and_adjoint": round(dt, 3), "seconds_forward": round(dtf, 3),
+                     "grad_inlet_norm": float(np.linalg.norm(gi)), "grad_u0_norm": float(np.linalg.norm(gu))}
+        if prec == "f32":
+            g32 = (gi, gu)
+        else:
+            g64 = (gi, gu)
+    rl = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    out["f32_vs_f64_grad_rel_l2"] = {"inlet": rl(g32[0], g64[0]), "u0": rl(g32[1], g64[1])}
+    rng = np.random.default_rng(2026)
+    eps = 1e-3
+    errs = []
+    for _ in range(args.fd_directions):
+        di = rng.standard_normal(ui.shape)
+        du = rng.standard_normal(u0.shape)
+        sc = 1.0 / np.sqrt((di ** 2).sum() + (du ** 2).sum())
+        di, du = di * sc, du * sc
+        fd = (objective(prob, ui + eps * di, u0 + eps * du, "f64") -
+              objective(prob, ui - eps * di, u0 - eps * du, "f64")) / (2 * eps)
+        ad64 = float((g64[0] * di).sum() + (g64[1] * du).sum())
+        ad32 = float((g32[0] * di).sum() + (g32[1] * du).sum())
+        errs.append((abs(ad64 - fd) / abs(fd), abs(ad32 - fd) / abs(fd)))
+    e = np.array(errs)
+    out["central_differences"] = {"directions": len(errs), "eps": eps,
+                                  "max_rel_err_f64_adjoint": float(e[:, 0].max()),
+                                  "max_rel_err_f32_adjoint": float(e[:, 1].max()),
+                                  "median_rel_err_f64_adjoint": float(np.median(e[:, 0]))}
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -471,9 +531,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default=None,
                     help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
-    ap.add_argument("--study", default=None, choices=["precision", "batch"],
+    ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint"],
                     help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage; "
-                         "batch: 64 uneven Hybrid(B0) ducts in one persistent launch per step")
+                         "batch: 64 uneven Hybrid(B0) ducts in one persistent launch per step; "
+                         "adjoint: drag gradient of the 128x64x64 duct against central differences")
+    ap.add_argument("--fd-directions", type=int, default=32)
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--tgv-n", type=int, default=512)
@@ -506,6 +568,9 @@ def main():
         return
     if args.study == "batch":
         batch_study(args, torch)
+        return
+    if args.study == "adjoint":
+        adjoint_study(args, torch)
         return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)

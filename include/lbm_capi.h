@@ -216,7 +216,7 @@ typedef struct lbm_batch_tuning {
     int32_t threads;         /* threads per block (128 or 256) */
     int32_t blocks_per_sm;   /* persistent blocks per SM */
     int32_t even_unit;       /* two-cell vectors per work unit of the local step */
-    int32_t odd_unit;        /* row segments (of `threads` cells) per unit of the neighbour step */
+    int32_t odd_unit;        /* blocks of `threads` cells per unit of the neighbour step */
     float us_per_step;       /* measured by lbm_batch_tune: mean of one even + one odd launch / 2 */
 } lbm_batch_tuning;
 
@@ -242,6 +242,33 @@ int lbm_batch_synchronize(lbm_batch* b);
 int lbm_batch_enable_stats(lbm_batch* b, int enable);
 /* Synchronises and copies n x LBM_NSTAT doubles (instance-major). */
 int lbm_batch_get_stats(lbm_batch* b, double* out);
+
+/* ---- differentiation ---------------------------------------------------- */
+
+/* A duct problem for lbm_adjoint_run: the Legacy BGK duct step (inlet at x=0
+ * with a per-(y,z) velocity profile, zero-gradient outlet, halfway bounce-back
+ * on the mask, y and z periodic) from f^0 = feq(1, u0), n_steps steps, and the
+ * objective J = mean momentum-exchange drag (x) over the 1-based steps
+ * window_begin .. window_end. */
+typedef struct lbm_adj_problem {
+    int32_t nx, ny, nz;
+    double tau;                 /* double, so that FP64 runs see the exact rate */
+    double force[3];
+    int32_t n_steps;
+    int32_t window_begin, window_end;
+    int32_t checkpoint_every;   /* forward states kept every k steps, the rest recomputed */
+    int32_t precision;          /* 0: FP32, 1: FP64 (state, adjoint and arithmetic) */
+} lbm_adj_problem;
+
+/* Objective and, when grad_inlet / grad_u0 are not NULL, its gradient by the
+ * hand-written discrete adjoint of the step (reverse pass over checkpointed,
+ * recomputed forward states).  host_mask: Nx*Ny*Nz bytes as lbm_set_solid_mask
+ * takes them (walls 1|LBM_MASK_WALL are left out of the drag); u_inlet and
+ * grad_inlet: Ny*Nz values, index z*Ny + y; u0 and grad_u0: three planes of
+ * N values (u_x, u_y, u_z).  Synchronous; allocates its own device memory.  No
+ * reference counterpart (the reference has no inlet, drag or gradients). */
+int lbm_adjoint_run(const lbm_adj_problem* p, const uint8_t* host_mask, const double* u_inlet,
+                    const double* u0, double* objective, double* grad_inlet, double* grad_u0);
 
 /* ---- geometry (host in, host out) ------------------------------------- */
 

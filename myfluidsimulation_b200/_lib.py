@@ -50,6 +50,12 @@ class BatchTuning(C.Structure):
                 ("odd_unit", C.c_int32), ("us_per_step", C.c_float)]
 
 
+class AdjProblem(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32), ("tau", C.c_double),
+                ("force", C.c_double * 3), ("n_steps", C.c_int32), ("window_begin", C.c_int32),
+                ("window_end", C.c_int32), ("checkpoint_every", C.c_int32), ("precision", C.c_int32)]
+
+
 # (name, restype, argtypes)
 _P = C.c_void_p
 _PROTOS = [
@@ -89,6 +95,7 @@ _PROTOS = [
     ("lbm_batch_synchronize", C.c_int, [_P]),
     ("lbm_batch_enable_stats", C.c_int, [_P, C.c_int]),
     ("lbm_batch_get_stats", C.c_int, [_P, _P]),
+    ("lbm_adjoint_run", C.c_int, [C.POINTER(AdjProblem), _P, _P, _P, _P, _P, _P]),
     ("lbm_load_stl", C.c_int, [C.c_char_p, C.POINTER(_P), C.POINTER(C.c_int64), _P]),
     ("lbm_free", None, [_P]),
     ("lbm_voxelize", C.c_int, [_P, C.c_int64, _P, C.POINTER(VoxelParams), _P]),

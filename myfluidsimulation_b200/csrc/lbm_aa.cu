@@ -367,7 +367,7 @@ cudaError_t launch_typed(const AAParams& p, int parity, LaunchCfg cfg, cudaStrea
 // Batched step: many independent instances (each its own AAParams: grid,
 // populations, flags, rates, boundary) advanced by ONE persistent launch.  The
 // work is a list of units {instance, first, count, -}: even steps count
-// two-cell vectors, odd steps count row segments of blockDim.x cells.  Blocks
+// two-cell vectors, odd steps count cells.  Blocks
 // take units round-robin; with statistics each unit's FP64 sums go to its own
 // slot and batch_finalize adds the slots of each instance in order.
 // ---------------------------------------------------------------------------
@@ -398,9 +398,12 @@ template <class ST, int MODE>
 __global__ void __launch_bounds__(256, 2) aa_batch_even(const AAParams* __restrict__ inst, const int4* __restrict__ units,
                                                      int nunits, double* __restrict__ partials) {
     constexpr bool STATS = MODE == 2;
+    __shared__ AAParams p;   // the unit's instance, read by every thread (broadcast)
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const int4 w = units[u];
-        const AAParams p = inst[w.x];   // the fields the unit uses, in registers
+        __syncthreads();
+        if (threadIdx.x == 0) p = inst[w.x];
+        __syncthreads();
         double acc[NSTAT];
 #pragma unroll
         for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
@@ -414,17 +417,19 @@ template <class ST, int MODE>
 __global__ void __launch_bounds__(256, 4) aa_batch_odd(const AAParams* __restrict__ inst, const int4* __restrict__ units,
                                                        int nunits, double* __restrict__ partials) {
     constexpr bool STATS = MODE == 2;
+    __shared__ AAParams p;   // the unit's instance, read by every thread (broadcast)
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
         const int4 w = units[u];
-        const AAParams p = inst[w.x];   // the fields the unit uses, in registers
-        const int segs = (p.nx + (int)blockDim.x - 1) / (int)blockDim.x;
+        __syncthreads();
+        if (threadIdx.x == 0) p = inst[w.x];
+        __syncthreads();
         double acc[NSTAT];
 #pragma unroll
         for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-        for (int sg = w.y; sg < w.y + w.z; ++sg) {
-            const int row = sg / segs;
-            const int x = (sg - row * segs) * (int)blockDim.x + (int)threadIdx.x;
-            if (x < p.nx) odd_cell<ST, true, MODE, uint32_t>(p, (uint32_t)row, x, acc);
+        // consecutive cells across row ends, so narrow rows leave no thread idle
+        for (int c = w.y + (int)threadIdx.x; c < w.y + w.z; c += (int)blockDim.x) {
+            const int row = c / p.nx;
+            odd_cell<ST, true, MODE, uint32_t>(p, (uint32_t)row, c - row * p.nx, acc);
         }
         if constexpr (STATS) block_reduce_into(acc, partials + (size_t)u * NSTAT);
     }

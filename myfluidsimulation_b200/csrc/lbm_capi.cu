@@ -623,9 +623,8 @@ int batch_build_units(lbm_batch* b) {
         for (size_t i = 0; i < b->inst.size(); ++i) {
             const lbm_solver* s = b->inst[i];
             first.push_back((int)u.size());
-            const int64_t total = par == 0 ? s->N / 2
-                                           : (int64_t)((s->dom.nx + T - 1) / T) * s->dom.ny * s->dom.nz;
-            const int step = par == 0 ? E : O;
+            const int64_t total = par == 0 ? s->N / 2 : s->N;
+            const int step = par == 0 ? E : O * T;
             for (int64_t f = 0; f < total; f += step)
                 u.push_back(make_int4((int)i, (int)f, (int)std::min<int64_t>(step, total - f), 0));
         }

@@ -59,8 +59,7 @@ struct LaunchCfg {
 cudaError_t launch_aa_step(const AAParams& p, int storage, int parity, LaunchCfg cfg, cudaStream_t s);
 // One step of many instances in one persistent launch (FP32 populations, the
 // instances' flag bytes required); units: {instance, first, count, -} with
-// first/count in two-cell vectors (parity 0) or row segments of `threads`
-// cells (parity 1).  stats != 0 writes NSTAT sums per unit into partials.
+// first/count in two-cell vectors (parity 0) or cells (parity 1).  stats != 0 writes NSTAT sums per unit into partials.
 cudaError_t launch_aa_batch(const AAParams* d_inst, const int4* d_units, int nunits, int parity, int stats,
                             int storage, int blocks, int threads, double* partials, cudaStream_t s);
 // per-instance sums of the unit partials: units of instance i are first[i]..first[i+1]-1

@@ -139,6 +139,24 @@ int lbm_reinit_from_macro(lbm_solver* s, const float* d_rho, const float* d_ux,
 int lbm_reinit_from_host(lbm_solver* s, const float* rho, const float* ux,
                          const float* uy, const float* uz);
 
+/* Pipelined host I/O, for loops that feed every run from host memory and read
+ * its result back (host arrays should be pinned for the copies to overlap):
+ * lbm_stage_from_host copies the macro fields (NULL: as in
+ * lbm_reinit_from_macro) into one of two staging buffers on the solver's copy
+ * stream and returns at once; lbm_reinit_from_stage then reinitialises from
+ * the last staged fields on the compute stream, after that copy.  For
+ * Legacy/Hybrid it leaves the macro fields as they were (the next step
+ * rewrites them), so a read of the previous run's fields can still be in
+ * flight.  lbm_read_macros_async copies the current macro fields to host on
+ * the copy stream; the next call that rewrites them waits for it, and
+ * lbm_wait_reads (or lbm_synchronize of both streams) waits for it on the
+ * host.  No reference counterpart (the reference copies synchronously,
+ * src/bench/main_taylor_green.cpp:90-105,143-156). */
+int lbm_stage_from_host(lbm_solver* s, const float* rho, const float* ux, const float* uy, const float* uz);
+int lbm_reinit_from_stage(lbm_solver* s);
+int lbm_read_macros_async(lbm_solver* s, float* rho, float* ux, float* uy, float* uz);
+int lbm_wait_reads(lbm_solver* s);
+
 /* Advances `substeps` steps, asynchronously on the solver's stream.  The
  * macro fields (and, when enabled, the statistics) are those of the last
  * substep, as in the reference, where they hold the moments of the state the

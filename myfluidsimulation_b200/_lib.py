@@ -70,6 +70,10 @@ _PROTOS = [
     ("lbm_reset", C.c_int, [_P]),
     ("lbm_reinit_from_macro", C.c_int, [_P, _P, _P, _P, _P]),
     ("lbm_reinit_from_host", C.c_int, [_P, _P, _P, _P, _P]),
+    ("lbm_stage_from_host", C.c_int, [_P, _P, _P, _P, _P]),
+    ("lbm_reinit_from_stage", C.c_int, [_P]),
+    ("lbm_read_macros_async", C.c_int, [_P, _P, _P, _P, _P]),
+    ("lbm_wait_reads", C.c_int, [_P]),
     ("lbm_step", C.c_int, [_P, C.c_int]),
     ("lbm_step_graph", C.c_int, [_P, C.c_int]),
     ("lbm_synchronize", C.c_int, [_P]),

@@ -66,6 +66,15 @@ struct lbm_solver {
     // graph cache
     cudaGraphExec_t gexec = nullptr;
     int g_sub = 0, g_parity = -1, g_stats = -1;
+    // pipelined host I/O (lbm_stage_from_host, lbm_reinit_from_stage, lbm_read_macros_async)
+    cudaStream_t copy_stream = nullptr;
+    float* stage[2] = {nullptr, nullptr};
+    bool stage_has[2][4] = {};
+    int stage_next = 0, stage_ready = -1;
+    bool stage_inuse[2] = {false, false};
+    cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_stage_free[2] = {nullptr, nullptr};
+    cudaEvent_t ev_macros = nullptr, ev_read = nullptr;
+    bool read_pending = false;
 };
 
 namespace {
@@ -149,11 +158,25 @@ lbm::HomeParams home_params(lbm_solver* s, bool stats) {
 }  // namespace
 
 // queue n substeps (no sync)
+// an asynchronous read of the macro fields must finish before they are rewritten
+static int wait_pending_read(lbm_solver* s) {
+    if (s->read_pending) {
+        CK(cudaStreamWaitEvent(s->stream, s->ev_read, 0));
+        s->read_pending = false;
+    }
+    return LBM_OK;
+}
+
 static int enqueue_steps(lbm_solver* s, int n) {
     for (int i = 0; i < n; ++i) {
         const bool last = (i == n - 1);
         const bool st = last && s->stats_on;
         const bool mac = last && (s->macro_out || st);
+        // HOME's macro fields are its state: every step rewrites one of the two buffers
+        if (mac || !is_aa(s)) {
+            const int rc = wait_pending_read(s);
+            if (rc != LBM_OK) return rc;
+        }
         if (is_ref_push(s)) {
             lbm::AAParams p = aa_params(s, mac, st);
             CK(lbm::launch_ref_push(p, static_cast<const float*>(cur_pop(s)), static_cast<float*>(other_pop(s)),
@@ -283,6 +306,12 @@ int lbm_destroy(lbm_solver* s) {
     cudaFree(s->f); cudaFree(s->f2); cudaFree(s->m[0]); cudaFree(s->m[1]); cudaFree(s->macro);
     cudaFree(s->mask); cudaFree(s->band); cudaFree(s->flags); cudaFree(s->links);
     cudaFree(s->dist); cudaFree(s->dcount); cudaFree(s->partials); cudaFree(s->stats);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+    cudaFree(s->stage[0]); cudaFree(s->stage[1]);
+    for (cudaEvent_t e : {s->ev_staged[0], s->ev_staged[1], s->ev_stage_free[0], s->ev_stage_free[1], s->ev_macros,
+                          s->ev_read})
+        if (e) cudaEventDestroy(e);
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return LBM_OK;
@@ -339,17 +368,29 @@ int lbm_get_band(lbm_solver* s, uint8_t* out) {
 
 int lbm_reset(lbm_solver* s) { return lbm_reinit_from_macro(s, nullptr, nullptr, nullptr, nullptr); }
 
+static int reinit_impl(lbm_solver* s, const float* d_rho, const float* d_ux, const float* d_uy, const float* d_uz,
+                       bool write_macros);
+
 int lbm_reinit_from_macro(lbm_solver* s, const float* d_rho, const float* d_ux, const float* d_uy,
                           const float* d_uz) {
     if (!s) { set_error("lbm_reinit_from_macro: null solver"); return LBM_ERR_INVALID; }
+    const int rc = wait_pending_read(s);
+    if (rc != LBM_OK) return rc;
+    return reinit_impl(s, d_rho, d_ux, d_uy, d_uz, true);
+}
+
+static int reinit_impl(lbm_solver* s, const float* d_rho, const float* d_ux, const float* d_uy, const float* d_uz,
+                       bool write_macros) {
     if (is_aa(s)) {
         // Legacy with no rho resets to rho=1, u=0 (legacy.cu:174-178): the same
         // state as feq(1, 0); Hybrid uses rho=1 and the given u (hybrid.cu:76-79).
         if (s->method == LBM_METHOD_LEGACY && !d_rho) d_ux = d_uy = d_uz = nullptr;
         const int form = s->method == LBM_METHOD_LEGACY ? (d_rho ? 0 : 1) : 1;
         void* dst = cur_pop(s);
-        CK(lbm::launch_aa_reinit(dst, s->storage, s->rho0, s->N, d_rho, d_ux, d_uy, d_uz, s->macro,
-                                 s->macro + s->N, s->macro + 2 * s->N, s->macro + 3 * s->N, form, s->stream));
+        float* mo = write_macros ? s->macro : nullptr;
+        CK(lbm::launch_aa_reinit(dst, s->storage, s->rho0, s->N, d_rho, d_ux, d_uy, d_uz, mo,
+                                 mo ? mo + s->N : nullptr, mo ? mo + 2 * s->N : nullptr, mo ? mo + 3 * s->N : nullptr,
+                                 form, s->stream));
         if (is_ref_push(s)) {
             // the reference's Legacy copies f into fnext after reinitialising
             // (legacy.cu:204-206); its reset (null rho) and Hybrid's reinit leave
@@ -374,6 +415,10 @@ int lbm_reinit_from_macro(lbm_solver* s, const float* d_rho, const float* d_ux, 
 
 int lbm_reinit_from_host(lbm_solver* s, const float* rho, const float* ux, const float* uy, const float* uz) {
     if (!s) { set_error("lbm_reinit_from_host: null solver"); return LBM_ERR_INVALID; }
+    {
+        const int rc = wait_pending_read(s);   // the macro buffers are the staging area here
+        if (rc != LBM_OK) return rc;
+    }
     // stage through the solver's own buffers: AA macro fields, or HOME's next buffer
     float* stage = is_aa(s) ? s->macro : nullptr;
     float* tmp = nullptr;
@@ -394,6 +439,85 @@ int lbm_reinit_from_host(lbm_solver* s, const float* rho, const float* ux, const
     const int rc = lbm_reinit_from_macro(s, dptr[0], dptr[1], dptr[2], dptr[3]);
     if (tmp) cudaFreeAsync(tmp, s->stream);
     return rc;
+}
+
+static int ensure_copy_path(lbm_solver* s) {
+    if (s->copy_stream) return LBM_OK;
+    CK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+        CK(cudaEventCreateWithFlags(&s->ev_staged[k], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&s->ev_stage_free[k], cudaEventDisableTiming));
+    }
+    CK(cudaEventCreateWithFlags(&s->ev_macros, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s->ev_read, cudaEventDisableTiming));
+    return LBM_OK;
+}
+
+int lbm_stage_from_host(lbm_solver* s, const float* rho, const float* ux, const float* uy, const float* uz) {
+    if (!s) { set_error("lbm_stage_from_host: null solver"); return LBM_ERR_INVALID; }
+    int rc = ensure_copy_path(s);
+    if (rc != LBM_OK) return rc;
+    const int k = s->stage_next;
+    if (!s->stage[k]) CK(cudaMalloc((void**)&s->stage[k], sizeof(float) * 4 * (size_t)s->N));
+    // the reinit that last read this buffer must be done with it
+    if (s->stage_inuse[k]) CK(cudaStreamWaitEvent(s->copy_stream, s->ev_stage_free[k], 0));
+    const float* src[4] = {rho, ux, uy, uz};
+    for (int c = 0; c < 4; ++c) {
+        s->stage_has[k][c] = src[c] != nullptr;
+        if (src[c])
+            CK(cudaMemcpyAsync(s->stage[k] + c * s->N, src[c], sizeof(float) * (size_t)s->N, cudaMemcpyHostToDevice,
+                               s->copy_stream));
+    }
+    CK(cudaEventRecord(s->ev_staged[k], s->copy_stream));
+    s->stage_ready = k;
+    s->stage_next ^= 1;
+    return LBM_OK;
+}
+
+int lbm_reinit_from_stage(lbm_solver* s) {
+    if (!s) { set_error("lbm_reinit_from_stage: null solver"); return LBM_ERR_INVALID; }
+    if (s->stage_ready < 0) { set_error("lbm_reinit_from_stage: nothing staged"); return LBM_ERR_INVALID; }
+    const int k = s->stage_ready;
+    CK(cudaStreamWaitEvent(s->stream, s->ev_staged[k], 0));
+    // Legacy/Hybrid leave the macro fields to the next step (so a read of the
+    // previous step's fields may still be in flight); HOME's state is rewritten
+    if (!is_aa(s)) {
+        const int rc = wait_pending_read(s);
+        if (rc != LBM_OK) return rc;
+    }
+    const float* d[4];
+    for (int c = 0; c < 4; ++c) d[c] = s->stage_has[k][c] ? s->stage[k] + c * s->N : nullptr;
+    const int rc = reinit_impl(s, d[0], d[1], d[2], d[3], !is_aa(s));
+    if (rc != LBM_OK) return rc;
+    CK(cudaEventRecord(s->ev_stage_free[k], s->stream));
+    s->stage_inuse[k] = true;
+    s->stage_ready = -1;
+    return LBM_OK;
+}
+
+int lbm_read_macros_async(lbm_solver* s, float* rho, float* ux, float* uy, float* uz) {
+    if (!s) { set_error("lbm_read_macros_async: null solver"); return LBM_ERR_INVALID; }
+    int rc = ensure_copy_path(s);
+    if (rc != LBM_OK) return rc;
+    rc = wait_pending_read(s);   // one read in flight at a time
+    if (rc != LBM_OK) return rc;
+    float* b = is_aa(s) ? s->macro : home_macro_base(s);
+    CK(cudaEventRecord(s->ev_macros, s->stream));
+    CK(cudaStreamWaitEvent(s->copy_stream, s->ev_macros, 0));
+    float* dst[4] = {rho, ux, uy, uz};
+    for (int c = 0; c < 4; ++c)
+        if (dst[c])
+            CK(cudaMemcpyAsync(dst[c], b + c * s->N, sizeof(float) * (size_t)s->N, cudaMemcpyDeviceToHost,
+                               s->copy_stream));
+    CK(cudaEventRecord(s->ev_read, s->copy_stream));
+    s->read_pending = true;
+    return LBM_OK;
+}
+
+int lbm_wait_reads(lbm_solver* s) {
+    if (!s) { set_error("lbm_wait_reads: null solver"); return LBM_ERR_INVALID; }
+    if (s->copy_stream) CK(cudaStreamSynchronize(s->copy_stream));
+    return LBM_OK;
 }
 
 int lbm_step(lbm_solver* s, int substeps) {
@@ -433,6 +557,7 @@ int lbm_step_graph(lbm_solver* s, int substeps) {
 int lbm_synchronize(lbm_solver* s) {
     if (!s) { set_error("lbm_synchronize: null solver"); return LBM_ERR_INVALID; }
     CK(cudaStreamSynchronize(s->stream));
+    if (s->copy_stream) CK(cudaStreamSynchronize(s->copy_stream));
     return LBM_OK;
 }
 

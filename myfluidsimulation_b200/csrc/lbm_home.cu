@@ -26,6 +26,8 @@
 //   * F16/BF16 moments are stored with stochastic rounding (cvt.rs).
 // DRAM traffic is the 10 moments read once and written once (80 B per cell in
 // FP32, 40 B in F16/BF16) plus the halo re-reads that L2 does not absorb.
+#include <type_traits>
+
 #include "lbm_common.cuh"
 #include "lbm_internal.h"
 
@@ -208,6 +210,32 @@ template <> struct MomStore<__nv_bfloat16> {
         *reinterpret_cast<uint32_t*>(p) = cvt_rs_bf16x2(a, b, sr_bits(a, b, salt));
     }
 };
+
+// The 10 new moments of one cell.  FP32 stores them as they are; F16/BF16
+// convert them two at a time with one stochastic-rounding conversion
+// (cvt.rs.*x2) and split the pair into the two planes, drawing the five random
+// words from one hash of the cell's index and first two values.
+template <class T, class IDX>
+__device__ __forceinline__ void store_moments(T* op, IDX N, float r0, const float (&out)[10], uint32_t salt) {
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int c = 0; c < 10; ++c) op[(IDX)c * N] = out[c];
+    } else {
+        constexpr bool F16 = std::is_same<T, __half>::value;
+        const float sc = F16 ? kF16Scale : 1.0f;
+        const uint32_t h = mix32(salt ^ __float_as_uint(out[0]) ^ (__float_as_uint(out[1]) * 0x9e3779b9u));
+        uint16_t* o = reinterpret_cast<uint16_t*>(op);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+            uint32_t rb = h * (2u * k + 1u) * 0x85ebca6bu;
+            rb ^= rb >> 15;
+            const float a = (k == 0 ? out[0] - r0 : out[2 * k]) * sc, b = out[2 * k + 1] * sc;
+            const uint32_t d = F16 ? cvt_rs_f16x2(a, b, rb) : cvt_rs_bf16x2(a, b, rb);
+            o[(IDX)(2 * k) * N] = (uint16_t)(d & 0xffffu);
+            o[(IDX)(2 * k + 1) * N] = (uint16_t)(d >> 16);
+        }
+    }
+}
 
 // A tile cell writes all 19 populations leaving its plane; a halo position
 // writes only the directions that point into the tile: dir 0 = x-1 column
@@ -402,7 +430,7 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
                                        Mxx - fmaf(rx, ux, r3), Mxy - rx * uy, Mxz - rx * uz,
                                        Myy - fmaf(ry, uy, r3), Myz - ry * uz, Mzz - fmaf(rz, uz, r3)};
 #pragma unroll
-                for (int c = 0; c < 10; ++c) MomStore<T>::st(op + (IDX)c * N, c, r0, out[c], (uint32_t)id * 10u + c);
+                store_moments<T, IDX>(op, N, r0, out, (uint32_t)id);
                 if (STATS) {
                     acc[0] += (double)r;
                     acc[1] += 0.5 * ((double)ux * ux + (double)uy * uy + (double)uz * uz);

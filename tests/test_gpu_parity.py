@@ -256,3 +256,77 @@ def test_periodic_mass_conservation_long(gpu):
     m1 = s.stats()["mass"]
     s.close()
     assert abs(m1 - m0) / m0 < 1e-5
+
+
+@pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HOME])
+def test_pipelined_host_io_matches_synchronous(gpu, method):
+    """lbm_stage_from_host / lbm_reinit_from_stage / lbm_read_macros_async give the
+    fields that lbm_reinit_from_host / lbm_step / lbm_get_macros give, run by run."""
+    import ctypes as C
+    from myfluidsimulation_b200._lib import check, lib
+    dims = (40, 18, 14)
+    nx, ny, nz = dims
+    mask = obstacle_mask(*dims, duct=True)
+    runs = [init_fields(*dims, seed=k) for k in range(3)]
+    L = lib()
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+
+    def solver():
+        s = Solver(*dims, 0.58, method=method, bc=BC_DUCT, inlet_u=0.05)
+        s.set_solid_mask(mask)
+        return s
+
+    s = solver()
+    want = []
+    for f in runs:
+        s.reinit_from_host(*f)
+        s.step(7)
+        want.append([x.copy() for x in s.macros()])
+    s.close()
+    s = solver()
+    host = [[np.ascontiguousarray(x, np.float32) for x in f] for f in runs]
+    outs = [[np.zeros((nz, ny, nx), np.float32) for _ in range(4)] for _ in range(3)]
+    check(L.lbm_stage_from_host(s._h, *[vp(x) for x in host[0]]))
+    for k in range(3):
+        check(L.lbm_reinit_from_stage(s._h))
+        if k + 1 < 3:
+            check(L.lbm_stage_from_host(s._h, *[vp(x) for x in host[k + 1]]))
+        check(L.lbm_step(s._h, 7))
+        check(L.lbm_read_macros_async(s._h, *[vp(o) for o in outs[k]]))
+    check(L.lbm_wait_reads(s._h))
+    s.synchronize()
+    s.close()
+    for k in range(3):
+        for a, b in zip(outs[k], want[k]):
+            np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("storage,tol", [(1, 5e-3), (2, 4e-2)])
+@pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HYBRID])
+@pytest.mark.parametrize("dims,bc", [((128, 12, 10), BC_DUCT), ((64, 10, 9), BC_PERIODIC), ((40, 9, 7), BC_PERIODIC)])
+def test_narrow_storage_vs_oracle(gpu, oracle, storage, tol, method, dims, bc):
+    """F16/BF16 populations (shifted, FP32 arithmetic) against the FP64 oracle.
+    Rows of 64 and 128 cells take the two-cells-per-thread odd step (warps with
+    a solid or boundary cell fall back to one cell per thread); 40 does not."""
+    nx, ny, nz = dims
+    duct = bc == BC_DUCT
+    mask = obstacle_mask(*dims, seed=3, duct=duct)
+    fields = init_fields(*dims, seed=4)
+    steps = 21
+    s = Solver(nx, ny, nz, 0.6, (0, 0, 0) if duct else (1e-5, 0, 0), method=method, storage=storage, bc=bc,
+               inlet_u=0.04)
+    s.set_solid_mask(mask)
+    s.reinit_from_host(*fields)
+    s.step(steps)
+    s.synchronize()
+    rho, u, v, w = s.macros()
+    s.close()
+    f0 = oracle.reinit_eq(*fields)
+    _, r_o, u_o, v_o, w_o, _ = oracle.bgk_run(f0, mask, steps, 0.6, (0, 0, 0) if duct else (1e-5, 0, 0),
+                                              mode=1 if method == METHOD_HYBRID else 0, bc=1 if duct else 0,
+                                              u_in=0.04, band=np.zeros_like(mask) if method == METHOD_HYBRID else None)
+    fl = mask == 0
+    e_u = vel_err([u[fl], v[fl], w[fl]], [u_o[fl], v_o[fl], w_o[fl]])
+    e_r = rl2(rho[fl] - 1.0, r_o[fl] - 1.0)
+    print(f"storage {storage} method {method} dims {dims}: u rel L2 {e_u:.3e}, rho-1 rel L2 {e_r:.3e}")
+    assert e_u < tol

@@ -172,6 +172,11 @@ int lbm_set_force(lbm_solver* s, float fx, float fy, float fz);
  * shear term.  The reference fixes it to 1/tau (lbm3d_hybrid.cu:264-267),
  * which is the default here too. */
 int lbm_set_shear_omega(lbm_solver* s, float omega_shear);
+/* HOME only: planes per block of the moment step (the z-chunk; 1..Nz, larger
+ * values are clamped to Nz).  A tuning knob with no reference counterpart:
+ * results do not depend on it.  lbm_create picks a value from the grid. */
+int lbm_set_home_zchunk(lbm_solver* s, int zchunk);
+int lbm_home_zchunk(lbm_solver* s, int* zchunk);
 
 /* Borrowed device pointers of the macro fields.  Replaces d_rho/d_u/d_v/d_w
  * (lbm3d_legacy.cu:229-236, lbm3d_home.cu:355-362, lbm3d_hybrid.hpp:45-52). */

@@ -79,6 +79,8 @@ _PROTOS = [
     ("lbm_synchronize", C.c_int, [_P]),
     ("lbm_set_force", C.c_int, [_P, C.c_float, C.c_float, C.c_float]),
     ("lbm_set_shear_omega", C.c_int, [_P, C.c_float]),
+    ("lbm_set_home_zchunk", C.c_int, [_P, C.c_int]),
+    ("lbm_home_zchunk", C.c_int, [_P, C.POINTER(C.c_int)]),
     ("lbm_macro_ptrs", C.c_int, [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
     ("lbm_get_macros", C.c_int, [_P, _P, _P, _P, _P]),
     ("lbm_get_state", C.c_int, [_P, _P]),

@@ -3,7 +3,7 @@
 ``python -m myfluidsimulation_b200.build`` compiles every source under csrc/
 with nvcc for ``sm_100a`` (``-gencode arch=compute_100a,code=sm_100a``) in
 parallel and links the shared library next to this file, plus the C++
-command-line tools under apps/ (fluidsim_legacy/home/hybrid/tgv) into bin/.
+command-line tools under apps/ (fluidsim_legacy/home/hybrid/tgv/sweep) into bin/.
 """
 from __future__ import annotations
 
@@ -27,7 +27,7 @@ NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=
 
 SOURCES = ["lbm_aa.cu", "lbm_push.cu", "lbm_home.cu", "lbm_aux.cu", "lbm_geom.cu", "lbm_capi.cu", "lbm_static.cu", "lbm_adjoint.cu", "lbm_io.cpp"]
 HEADERS = ["lbm_common.cuh", "lbm_internal.h"]
-APP_NAMES = ["fluidsim_legacy", "fluidsim_home", "fluidsim_hybrid", "fluidsim_tgv"]
+APP_NAMES = ["fluidsim_legacy", "fluidsim_home", "fluidsim_hybrid", "fluidsim_tgv", "fluidsim_sweep"]
 
 
 def nvcc() -> str:

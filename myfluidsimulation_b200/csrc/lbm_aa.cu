@@ -300,129 +300,6 @@ __global__ void __launch_bounds__(256, MASK ? 4 : 3) aa_odd(AAParams p) {
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }
 
-// the one-cell path, kept out of line in the paired kernel (rare there)
-template <class ST, bool MASK, int MODE, class IDX>
-__device__ __noinline__ void odd_cell_out_of_line(const AAParams& p, IDX row, int x, double* acc) {
-    double a[NSTAT];
-#pragma unroll
-    for (int k = 0; k < NSTAT; ++k) a[k] = 0.0;
-    odd_cell<ST, MASK, MODE, IDX>(p, row, x, a);
-#pragma unroll
-    for (int k = 0; k < NSTAT; ++k) acc[k] += a[k];
-}
-
-// Odd step for 2-byte storage (F16/BF16), two cells per thread.  A warp holds
-// 64 consecutive cells of one row: the populations that cross x between its
-// cells travel through warp shuffles, so every global access is a 4-byte pair
-// (128 B per warp instruction) instead of a 2-byte scalar.  Lanes 0 and 31
-// read and write the one value beyond the warp's cells directly.  A warp with a
-// solid cell, a non-streaming link or cells past the row end runs odd_cell for
-// each of its cells instead.  Requires nx even.
-template <class ST, bool MASK, int MODE, class IDX>
-__global__ void __launch_bounds__(256, 2) aa_odd_pair(AAParams p) {
-    constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
-    constexpr unsigned FULL = 0xffffffffu;
-    using T = typename ST::T;
-    T* __restrict__ f = static_cast<T*>(p.f);
-    const IDX N = (IDX)p.N;
-    const int nx = p.nx, ny = p.ny, nz = p.nz;
-    const int seg = 2 * (int)blockDim.x;
-    const int segs = (nx + seg - 1) / seg;
-    const IDX total = (IDX)segs * ny * nz;
-    const int lane = threadIdx.x & 31;
-    const float r0 = p.rho0;
-    double acc[NSTAT];
-#pragma unroll
-    for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-
-    for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
-        const IDX row = sg / segs;
-        const int x = (int)(sg - row * segs) * seg + 2 * (int)threadIdx.x;
-        const int xw = x - 2 * lane;                    // the warp's first cell
-        const bool valid = x < nx;
-        const IDX id = row * nx + x;
-        bool slow = xw + 64 > nx;                        // warp-uniform
-        if (!slow && MASK) {
-            const uint32_t f2 = *reinterpret_cast<const uint16_t*>(p.flags + id);
-            slow = __any_sync(FULL, (f2 & 0xffu & (F_SOLID | F_SPECIAL)) || ((f2 >> 8) & (F_SOLID | F_SPECIAL)));
-        }
-        if (slow) {
-            for (int k = 0; k < 2; ++k)
-                if (x + k < nx) odd_cell_out_of_line<ST, MASK, MODE, IDX>(p, row, x + k, acc);
-            continue;
-        }
-        const int y = (int)(row % ny);
-        const int z = (int)(row / ny);
-        Nbr<IDX> nb;
-        nb.init(x, y, z, nx, ny, nz);
-        const int xl = x == 0 ? nx - 1 : x - 1;         // lane 0's left neighbour (periodic x here)
-        const int xr = x + 2 >= nx ? x + 2 - nx : x + 2; // lane 31's right neighbour
-        float a[19], b[19];
-#pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            const T* base = f + (IDX)opp(q) * N + nb.r[1 - cy(q)][1 - cz(q)];
-            float v[2];
-            ST::ld2(base + x, opp(q), r0, v);
-            if (cx(q) == 0) {
-                a[q] = v[0]; b[q] = v[1];
-            } else if (cx(q) > 0) {            // sources x-1, x
-                b[q] = v[0];
-                a[q] = __shfl_up_sync(FULL, v[1], 1);
-                if (lane == 0) a[q] = ST::ld(base + xl, opp(q), r0);
-            } else {                                     // sources x+1, x+2
-                a[q] = v[1];
-                b[q] = __shfl_down_sync(FULL, v[0], 1);
-                if (lane == 31) b[q] = ST::ld(base + xr, opp(q), r0);
-            }
-        }
-        const Cell ma = moments(a, p.fx, p.fy, p.fz);
-        const Cell mb = moments(b, p.fx, p.fy, p.fz);
-        uint32_t fl2 = 0;
-        if (MASK) fl2 = *reinterpret_cast<const uint16_t*>(p.flags + id);
-        const float oma = (p.hybrid && !(fl2 & F_BAND)) ? p.omega_s : p.omega;
-        const float omb = (p.hybrid && !((fl2 >> 8) & F_BAND)) ? p.omega_s : p.omega;
-        collide(a, ma, oma);
-        collide(b, mb, omb);
-#pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            T* base = f + (IDX)q * N + nb.r[1 + cy(q)][1 + cz(q)];
-            if (cx(q) == 0) {
-                const float v[2] = {a[q], b[q]};
-                ST::st2(base + x, q, r0, v);
-            } else if (cx(q) > 0) {            // destinations x+1, x+2
-                const float up = __shfl_up_sync(FULL, b[q], 1);
-                if (lane == 0) {
-                    ST::st(base + x + 1, q, r0, a[q]);
-                } else {
-                    const float v[2] = {up, a[q]};
-                    ST::st2(base + x, q, r0, v);
-                }
-                if (lane == 31) ST::st(base + xr, q, r0, b[q]);
-            } else {                                     // destinations x-1, x
-                const float down = __shfl_down_sync(FULL, a[q], 1);
-                if (lane == 31) {
-                    ST::st(base + x, q, r0, b[q]);
-                } else {
-                    const float v[2] = {b[q], down};
-                    ST::st2(base + x, q, r0, v);
-                }
-                if (lane == 0) ST::st(base + xl, q, r0, a[q]);
-            }
-        }
-        if (MACRO) {
-            *reinterpret_cast<float2*>(p.rho + id) = make_float2(ma.r, mb.r);
-            *reinterpret_cast<float2*>(p.ux + id) = make_float2(ma.ux, mb.ux);
-            *reinterpret_cast<float2*>(p.uy + id) = make_float2(ma.uy, mb.uy);
-            *reinterpret_cast<float2*>(p.uz + id) = make_float2(ma.uz, mb.uz);
-        }
-        if (STATS) {
-            add_cell_stats(acc, ma);
-            add_cell_stats(acc, mb);
-        }
-    }
-    if constexpr (STATS) block_reduce_stats(acc, p.partials);
-}
-
 // The natural-layout populations f^n (the reference's d_f after n steps).
 template <class ST>
 __global__ void aa_materialize(AAParams p, int parity, float* __restrict__ out) {
@@ -466,13 +343,6 @@ void launch_mode(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
         } else {
             if (mask) aa_even<ST, true, 1, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
             else aa_even<ST, false, 1, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
-        }
-    } else if (ST::kId != 0 && p.nx % 64 == 0) {
-        // 2-byte storage: two cells per thread, one warp per 64 cells of a row
-        if constexpr (ST::kId != 0) {
-            const int threads = p.nx / 2 >= 256 ? 256 : p.nx / 2;
-            if (mask) aa_odd_pair<ST, true, MODE, IDX><<<cfg.blocks, threads, 0, s>>>(p);
-            else aa_odd_pair<ST, false, MODE, IDX><<<cfg.blocks, threads, 0, s>>>(p);
         }
     } else {
         if (mask) aa_odd<ST, true, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);

@@ -257,11 +257,17 @@ int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out)
     const int sms = lbm::num_sms();
     s->cfg_even = {sms * 8, 256};
     s->cfg_odd = {sms * 12, 256};
-    // HOME: enough z-chunks to fill the chip a few times
+    // HOME: the longest z-chunk (fewest re-built halo planes) that still gives
+    // three waves of blocks at 3 blocks per SM, so the tail of the last wave
+    // stays short (measured on B200: 256x128x128 best at 12, 512^3 at 48)
     {
-        const int tiles = ((dom->nx + 31) / 32) * ((dom->ny + 7) / 8);
-        int zc = 32;
-        while (zc > 4 && (int64_t)tiles * ((dom->nz + zc - 1) / zc) < (int64_t)sms * 6) zc /= 2;
+        int zc = 4;
+        for (int c : {48, 32, 24, 16, 12, 10, 8, 6, 4}) {
+            if ((int64_t)lbm::home_num_blocks(dom->nx, dom->ny, dom->nz, std::min(c, dom->nz)) >= (int64_t)sms * 9) {
+                zc = c;
+                break;
+            }
+        }
         s->home_zchunk = std::min(zc, dom->nz);
     }
     s->max_blocks = std::max({s->cfg_even.blocks, s->cfg_odd.blocks,
@@ -573,6 +579,35 @@ int lbm_set_shear_omega(lbm_solver* s, float omega_shear) {
     if (s->method != LBM_METHOD_HYBRID) { set_error("lbm_set_shear_omega: Hybrid only"); return LBM_ERR_INVALID; }
     s->omega_s = omega_shear;
     drop_graph(s);
+    return LBM_OK;
+}
+
+int lbm_set_home_zchunk(lbm_solver* s, int zchunk) {
+    if (!s) { set_error("lbm_set_home_zchunk: null solver"); return LBM_ERR_INVALID; }
+    if (s->method != LBM_METHOD_HOME) { set_error("lbm_set_home_zchunk: HOME only"); return LBM_ERR_INVALID; }
+    if (zchunk < 1) { set_error("lbm_set_home_zchunk: zchunk must be >= 1"); return LBM_ERR_INVALID; }
+    const int z = std::min(zchunk, s->dom.nz);
+    const int need = lbm::home_num_blocks(s->dom.nx, s->dom.ny, s->dom.nz, z);
+    if (need > s->max_blocks) {
+        // per-block statistics partials: grow once the step queue has drained
+        CK(cudaStreamSynchronize(s->stream));
+        double* p = nullptr;
+        if (cudaMalloc((void**)&p, sizeof(double) * lbm::NSTAT * (size_t)need) != cudaSuccess) {
+            set_error("lbm_set_home_zchunk: device allocation failed");
+            return LBM_ERR_ALLOC;
+        }
+        cudaFree(s->partials);
+        s->partials = p;
+        s->max_blocks = need;
+    }
+    s->home_zchunk = z;
+    drop_graph(s);
+    return LBM_OK;
+}
+
+int lbm_home_zchunk(lbm_solver* s, int* zchunk) {
+    if (!s || !zchunk) { set_error("lbm_home_zchunk: null argument"); return LBM_ERR_INVALID; }
+    *zchunk = s->home_zchunk;
     return LBM_OK;
 }
 

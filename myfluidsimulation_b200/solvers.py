@@ -125,6 +125,16 @@ class Solver:
     def set_shear_omega(self, omega_s):
         check(lib().lbm_set_shear_omega(self._h, float(omega_s)))
 
+    @property
+    def home_zchunk(self):
+        z = C.c_int()
+        check(lib().lbm_home_zchunk(self._h, C.byref(z)))
+        return z.value
+
+    @home_zchunk.setter
+    def home_zchunk(self, zchunk):
+        check(lib().lbm_set_home_zchunk(self._h, int(zchunk)))
+
     def enable_stats(self, on=True):
         check(lib().lbm_enable_stats(self._h, 1 if on else 0))
 

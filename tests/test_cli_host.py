@@ -84,3 +84,20 @@ def test_bad_numbers_fail_like_the_reference(tools, ref_parse, argv):
     assert ref_parse(argv, 0) is None
     r = subprocess.run([tool("fluidsim_legacy"), "--print-config"] + argv, capture_output=True, text=True)
     assert r.returncode != 0
+
+
+def test_sweep_tool_args_lines(tools):
+    """fluidsim_sweep prints fluidsim_compare's [args]/[amr ] lines (src/main_compare.cpp:312-315) and,
+    without --hybrid-sweep-max, exits 1 before touching a GPU (the viewer is not provided)."""
+    import numpy as np
+    f = lambda x: float(np.float32(x))
+    argv = ["--init", "gauss", "--amp", "0.01", "--center", "0.1", "0.2", "0.3", "--axis", "y", "--width", "0.4",
+            "--force", "2e-5", "--force-z", "-3e-6", "--amr", "--amr-threshold", "1.7"]
+    r = subprocess.run([tool("fluidsim_sweep")] + argv, capture_output=True, text=True)
+    assert r.returncode == 1
+    want = ["[args] init=%s amp=%.3g sigma=%.3g center=(%.3f,%.3f,%.3f) axis=%d width=%.3f forceX=%.3g"
+            % ("gauss", f(0.01), f(0.08), f(0.1), f(0.2), f(0.3), 1, f(0.4), f(2e-5)),
+            "[args] force=(%.3g, %.3g, %.3g)" % (f(2e-5), 0.0, f(-3e-6)),
+            "[amr ] refine=%d threshold=%.2f" % (2, 1.0)]
+    assert r.stdout.split("\n")[:3] == want
+    assert "--hybrid-sweep-max" in r.stderr

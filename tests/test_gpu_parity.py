@@ -11,7 +11,7 @@ import pytest
 
 from myfluidsimulation_b200 import workloads as W
 from myfluidsimulation_b200.solvers import (BC_DUCT, BC_PERIODIC, BOUNCE_HALFWAY, BOUNCE_REFERENCE, METHOD_HOME,
-                                            METHOD_HYBRID, METHOD_LEGACY, Solver)
+                                            METHOD_HYBRID, METHOD_LEGACY, STORE_F16, STORE_F32, Solver)
 
 pytestmark = pytest.mark.gpu
 
@@ -103,6 +103,33 @@ def test_legacy_vs_oracle(gpu, oracle, dims, tau, steps, with_mask, force, bounc
     assert rl2(g["state"], f) < TOL_F
     assert rl2(g["macros"][0], mac[0]) < TOL_F
     assert vel_err(g["macros"][1:], mac[1:]) < TOL_F
+
+
+@pytest.mark.parametrize("storage", [STORE_F32, STORE_F16])
+def test_home_zchunk_does_not_change_results(gpu, storage):
+    """The z-chunk only splits the planes among blocks: every chunk length gives the same bits."""
+    dims = (40, 20, 23)
+    fields = init_fields(*dims, seed=11)
+    mask = obstacle_mask(*dims, seed=12)
+    out = []
+    for zc in (None, 1, 5, 23, 100):
+        s = Solver(*dims, 0.6, (1e-5, 0, 0), method=METHOD_HOME, storage=storage)
+        if zc is not None:
+            s.home_zchunk = zc
+            assert s.home_zchunk == min(zc, dims[2])
+        s.set_solid_mask(mask)
+        s.reinit_from_host(*fields)
+        s.enable_stats(True)
+        s.step(9)
+        s.synchronize()
+        out.append((s.state(), s.stats()))
+        s.close()
+    for st, sts in out[1:]:
+        np.testing.assert_array_equal(st, out[0][0])
+        for k in ("mass", "ke_sum"):
+            assert abs(sts[k] - out[0][1][k]) <= 1e-12 * abs(out[0][1][k])
+    with pytest.raises(RuntimeError):
+        Solver(*dims, 0.6, method=METHOD_LEGACY).home_zchunk = 4
 
 
 def test_legacy_split_calls_match_one_call(gpu):
@@ -303,11 +330,11 @@ def test_pipelined_host_io_matches_synchronous(gpu, method):
 
 @pytest.mark.parametrize("storage,tol", [(1, 5e-3), (2, 4e-2)])
 @pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HYBRID])
-@pytest.mark.parametrize("dims,bc", [((128, 12, 10), BC_DUCT), ((64, 10, 9), BC_PERIODIC), ((40, 9, 7), BC_PERIODIC)])
+@pytest.mark.parametrize("dims,bc", [((128, 12, 10), BC_DUCT), ((64, 10, 9), BC_PERIODIC), ((42, 9, 7), BC_PERIODIC)])
 def test_narrow_storage_vs_oracle(gpu, oracle, storage, tol, method, dims, bc):
-    """F16/BF16 populations (shifted, FP32 arithmetic) against the FP64 oracle.
-    Rows of 64 and 128 cells take the two-cells-per-thread odd step (warps with
-    a solid or boundary cell fall back to one cell per thread); 40 does not."""
+    """F16/BF16 populations (shifted, FP32 arithmetic) against the FP64 oracle:
+    duct and periodic grids; cell counts divisible by 4 (four cells per thread
+    in the even step) and not (42x9x7: two cells per thread)."""
     nx, ny, nz = dims
     duct = bc == BC_DUCT
     mask = obstacle_mask(*dims, seed=3, duct=duct)

@@ -539,6 +539,141 @@ def adjoint_study(args, torch):
     print(json.dumps(out))
 
 
+def vtk_study(args, torch):
+    """VTK snapshots of the bench duct (256x128x128, Legacy): rho, |u| and u,
+    the three files the command-line tools write every --vtk-every steps.
+    (a) the reference's own writer (src/moment_vtk_writer.cu, built into
+        oracle/_ref: cudaMemcpy + ofstream) and its launch_speed, one snapshot;
+    (b) the library's synchronous writers (text formatted on the GPU);
+    (c) the asynchronous writer in a step loop: the loop's time with a snapshot
+        every --vtk-every steps minus the same loop without, per snapshot, and
+        the wait for the last file at the end;
+    (d) the formatting kernels alone (CUDA events), with their algorithmic bytes
+        (fields read + text written) against the measured HBM copy peak.
+    The first snapshot of (b) must be byte-identical to (a)'s files."""
+    import ctypes as C
+    import shutil
+    from myfluidsimulation_b200 import lib
+    from myfluidsimulation_b200.vtk import VTK_SCALAR, VTK_SPEED, VTK_VECTOR, VtkWriter
+    L = lib()
+    st = torch.cuda.current_stream()
+    with tempfile.TemporaryDirectory() as td:
+        mask, _, _ = build_mask(td)
+    s, _ = make_solver("legacy", mask, st.cuda_stream)
+    s.step(50)
+    torch.cuda.synchronize()
+    N = NX * NY * NZ
+    r, u, v, w = s.macro_ptrs()
+    speed = torch.empty(N, device="cuda")
+    out = {"study": "vtk", "workload": f"duct {NX}x{NY}x{NZ} Legacy after 50 steps; rho, |u| and u per snapshot"}
+    root = tempfile.mkdtemp(prefix="vtk_study_")
+    try:
+        def files(tag):
+            d = os.path.join(root, tag)
+            os.makedirs(d, exist_ok=True)
+            return [os.path.join(d, f"{k}.vtk").encode() for k in ("rho", "speed", "vel")]
+
+        # the baseline leg: the reference's own writer, built from its sources
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_bind import RefCUDA
+        ref_files = None
+        if RefCUDA.available():
+            R = C.CDLL(RefCUDA.path)
+            f = files("ref")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            R.launch_speed(C.c_void_p(u), C.c_void_p(v), C.c_void_p(w), C.c_void_p(speed.data_ptr()), C.c_int(N))
+            R.write_scalar_vtk(f[0], C.c_void_p(r), NX, NY, NZ)
+            R.write_scalar_vtk(f[1], C.c_void_p(speed.data_ptr()), NX, NY, NZ)
+            R.write_vector_vtk(f[2], C.c_void_p(u), C.c_void_p(v), C.c_void_p(w), NX, NY, NZ)
+            out["reference_writer_s_per_snapshot"] = round(time.perf_counter() - t0, 3)
+            out["cpu_baseline"] = {"kind": "reference", "cores": 1,
+                                   "sample": "one snapshot: src/moment_vtk_writer.cu (cudaMemcpy + ofstream <<) "
+                                             "and launch_speed, built into oracle/_ref"}
+            ref_files = f
+        else:
+            out["reference_writer_s_per_snapshot"] = None
+        times = []
+        for k in range(3):
+            f = files(f"sync{k}")
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            L.launch_speed(u, v, w, speed.data_ptr(), N)
+            assert L.lbm_write_scalar_vtk(f[0], r, NX, NY, NZ) == 0
+            assert L.lbm_write_scalar_vtk(f[1], speed.data_ptr(), NX, NY, NZ) == 0
+            assert L.lbm_write_vector_vtk(f[2], u, v, w, NX, NY, NZ) == 0
+            times.append(time.perf_counter() - t0)
+            if k == 0:
+                out["text_bytes_per_snapshot"] = sum(os.path.getsize(x) for x in f)
+                if ref_files:
+                    out["bytes_identical_to_reference"] = all(
+                        open(a, "rb").read() == open(b, "rb").read() for a, b in zip(f, ref_files))
+            shutil.rmtree(os.path.dirname(f[0]))
+        out["sync_gpu_writer_s_per_snapshot"] = round(statistics.median(times), 4)
+        if out["reference_writer_s_per_snapshot"]:
+            out["sync_speedup_vs_reference_writer"] = round(out["reference_writer_s_per_snapshot"] /
+                                                            out["sync_gpu_writer_s_per_snapshot"], 1)
+        # (c) asynchronous snapshots inside the step loop
+        steps, every = args.vtk_steps, args.vtk_every
+        s.step(10)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            s.step(1)
+        torch.cuda.synchronize()
+        plain = time.perf_counter() - t0
+        with VtkWriter(NX, NY, NZ, depth=3) as wr:
+            nsnap = 0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for k in range(1, steps + 1):
+                s.step(1)
+                if k % every == 0:
+                    f = files(f"async{nsnap}")
+                    rr, uu, vv, ww = s.macro_ptrs()
+                    wr.submit(VTK_SCALAR, f[0].decode(), rr, stream=s.stream)
+                    wr.submit(VTK_SPEED, f[1].decode(), uu, vv, ww, stream=s.stream)
+                    wr.submit(VTK_VECTOR, f[2].decode(), uu, vv, ww, stream=s.stream)
+                    nsnap += 1
+            torch.cuda.synchronize()
+            loop = time.perf_counter() - t0
+            wr.flush()
+            done = time.perf_counter() - t0
+            written = wr.bytes_written
+        out["async"] = {"steps": steps, "every": every, "snapshots": nsnap, "loop_s_without": round(plain, 4),
+                        "loop_s_with": round(loop, 4),
+                        "loop_overhead_ms_per_snapshot": round(1e3 * (loop - plain) / max(nsnap, 1), 2),
+                        "all_files_written_s": round(done, 4), "bytes_written": written}
+        # (d) the formatting kernels alone
+        text = torch.empty(int(L.lbm_vtk_text_bound(VTK_VECTOR, N)), dtype=torch.uint8, device="cuda")
+        peak, peak_kind = measured_peaks()
+        kern = {}
+        for name, kind, ptrs, nin in (("rho", VTK_SCALAR, (r, None, None), 1), ("speed", VTK_SPEED, (u, v, w), 3),
+                                      ("vel", VTK_VECTOR, (u, v, w), 3)):
+            ln = C.c_int64()
+            ts = []
+            for it in range(6):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                assert L.lbm_vtk_format(kind, *[None if p is None else C.c_void_p(p) for p in ptrs], N,
+                                        text.data_ptr(), text.numel(), C.byref(ln), st.cuda_stream) == 0
+                e1.record(st)
+                torch.cuda.synchronize()
+                if it >= 2:
+                    ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            gbs = (4 * nin * N + ln.value) / (ms * 1e-3) / 1e9
+            kern[name] = {"ms": round(ms, 3), "text_bytes": ln.value, "gvalues_per_s": round(nin * N / ms / 1e6, 2),
+                          "gb_s": round(gbs, 1), "frac_of_hbm": round(gbs / peak, 3) if peak else None}
+        out["format_kernels"] = kern
+        out["hbm_peak_gbs"] = {"value": peak, "source": peak_kind}
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+        s.close()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -549,10 +684,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default=None,
                     help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
-    ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint"],
+    ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint", "vtk"],
                     help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage; "
                          "batch: 64 uneven Hybrid(B0) ducts in one persistent launch per step; "
-                         "adjoint: drag gradient of the 128x64x64 duct against central differences")
+                         "adjoint: drag gradient of the 128x64x64 duct against central differences; "
+                         "vtk: snapshot cost of the GPU VTK writers against the reference's writer")
+    ap.add_argument("--vtk-steps", type=int, default=1000)
+    ap.add_argument("--vtk-every", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--batch-steps", type=int, default=2000)
@@ -589,6 +727,9 @@ def main():
         return
     if args.study == "adjoint":
         adjoint_study(args, torch)
+        return
+    if args.study == "vtk":
+        vtk_study(args, torch)
         return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)

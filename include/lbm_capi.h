@@ -344,6 +344,39 @@ int lbm_write_scalar_vtk(const char* filename, const float* d_field, int Nx, int
 int lbm_write_vector_vtk(const char* filename, const float* d_fx, const float* d_fy,
                          const float* d_fz, int Nx, int Ny, int Nz);
 
+/* ---- VTK text on the GPU, asynchronous writer --------------------------- */
+
+/* Line kinds: "v\n" of a scalar field, "|u|\n" computed from (u, v, w) as
+ * launch_speed does, "u v w\n" of a vector field.  Values are printed as the
+ * reference's `ofstream << float` prints them (src/moment_vtk_writer.cu:22,46). */
+enum { LBM_VTK_SCALAR = 0, LBM_VTK_SPEED = 1, LBM_VTK_VECTOR = 2 };
+/* Bytes a text buffer needs for n lines of `kind` (no header). */
+int64_t lbm_vtk_text_bound(int32_t kind, int64_t n);
+/* Formats n lines into device memory d_text (cap bytes, >= lbm_vtk_text_bound)
+ * on `stream`, synchronises the stream and returns the text length in *len. */
+int lbm_vtk_format(int32_t kind, const float* d_a, const float* d_b, const float* d_c, int64_t n,
+                   char* d_text, int64_t cap, int64_t* len, void* stream);
+/* Writes whole VTK files (header + text) in the background.  submit queues
+ * the formatting on `stream` (after the work already queued there, e.g. the
+ * step that produced the fields) and returns; a writer thread copies the text
+ * to pinned host memory and writes the file.  At most `depth` fields are in
+ * flight; submit waits for a free one.  flush waits for every queued file and
+ * returns the first error since the last flush.  No reference counterpart: the
+ * reference formats on the host, synchronously. */
+typedef struct lbm_vtk_writer lbm_vtk_writer;
+int lbm_vtk_writer_create(int32_t nx, int32_t ny, int32_t nz, int32_t depth, lbm_vtk_writer** out);
+int lbm_vtk_writer_submit(lbm_vtk_writer* w, int32_t kind, const float* d_a, const float* d_b,
+                          const float* d_c, const char* path, void* stream);
+int lbm_vtk_writer_flush(lbm_vtk_writer* w);
+/* Bytes written to files so far (headers included). */
+int lbm_vtk_writer_bytes(lbm_vtk_writer* w, uint64_t* bytes);
+int lbm_vtk_writer_destroy(lbm_vtk_writer* w);
+/* The same formatting on the host, for checks: value i's text at out + i*stride
+ * (stride >= 12), its length in lens[i]. */
+int lbm_format_g6(const float* v, int64_t n, char* out, int32_t stride, uint8_t* lens);
+/* The CUDA stream a solver runs on (cudaStream_t). */
+int lbm_solver_stream(lbm_solver* s, void** stream);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -19,6 +19,7 @@ ERRORS = {1: "LBM_ERR_INVALID", 2: "LBM_ERR_CUDA", 3: "LBM_ERR_ALLOC", 4: "LBM_E
 
 METHOD_LEGACY, METHOD_HOME, METHOD_HYBRID = 0, 1, 2
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+VTK_SCALAR, VTK_SPEED, VTK_VECTOR = 0, 1, 2
 BC_PERIODIC, BC_DUCT = 0, 1
 BOUNCE_HALFWAY, BOUNCE_REFERENCE = 0, 1
 NSTAT = 8
@@ -114,6 +115,15 @@ _PROTOS = [
     ("write_vector_vtk", None, [C.c_char_p, _P, _P, _P, C.c_int, C.c_int, C.c_int]),
     ("lbm_write_scalar_vtk", C.c_int, [C.c_char_p, _P, C.c_int, C.c_int, C.c_int]),
     ("lbm_write_vector_vtk", C.c_int, [C.c_char_p, _P, _P, _P, C.c_int, C.c_int, C.c_int]),
+    ("lbm_vtk_text_bound", C.c_int64, [C.c_int32, C.c_int64]),
+    ("lbm_vtk_format", C.c_int, [C.c_int32, _P, _P, _P, C.c_int64, _P, C.c_int64, C.POINTER(C.c_int64), _P]),
+    ("lbm_vtk_writer_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P)]),
+    ("lbm_vtk_writer_submit", C.c_int, [_P, C.c_int32, _P, _P, _P, C.c_char_p, _P]),
+    ("lbm_vtk_writer_flush", C.c_int, [_P]),
+    ("lbm_vtk_writer_bytes", C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    ("lbm_vtk_writer_destroy", C.c_int, [_P]),
+    ("lbm_format_g6", C.c_int, [_P, C.c_int64, _P, C.c_int32, _P]),
+    ("lbm_solver_stream", C.c_int, [_P, C.POINTER(_P)]),
 ]
 
 EXPORTED = [n for n, _, _ in _PROTOS]

@@ -242,17 +242,24 @@ inline int run(const Settings& s, int method, const char* tag) {
             vtk = false;
         }
     }
-    float* speed = nullptr;
-    if (vtk && cudaMalloc(&speed, sizeof(float) * (size_t)N) != cudaSuccess) return fail("speed buffer");
+    // snapshots: the text is formatted on the GPU, queued on the solver's
+    // stream behind the step, and written by the writer's thread while the
+    // next steps run (the reference formats on the host and waits)
+    lbm_vtk_writer* writer = nullptr;
+    void* stream = nullptr;
+    lbm_solver_stream(h, &stream);
+    if (vtk && lbm_vtk_writer_create(s.nx, s.ny, s.nz, 3, &writer) != LBM_OK) return fail("VTK writer");
     auto dump = [&](int step) {
         if (!vtk) return;
         float *r, *u, *v, *w;
-        lbm_synchronize(h);
         lbm_macro_ptrs(h, &r, &u, &v, &w);
-        launch_speed(u, v, w, speed, N);
-        write_scalar_vtk(vtk_file(dir, std::string("rho_") + tag, step).c_str(), r, s.nx, s.ny, s.nz);
-        write_scalar_vtk(vtk_file(dir, std::string("speed_") + tag, step).c_str(), speed, s.nx, s.ny, s.nz);
-        write_vector_vtk(vtk_file(dir, std::string("vel_") + tag, step).c_str(), u, v, w, s.nx, s.ny, s.nz);
+        const std::string f_rho = vtk_file(dir, std::string("rho_") + tag, step);
+        const std::string f_speed = vtk_file(dir, std::string("speed_") + tag, step);
+        const std::string f_vel = vtk_file(dir, std::string("vel_") + tag, step);
+        if (lbm_vtk_writer_submit(writer, LBM_VTK_SCALAR, r, nullptr, nullptr, f_rho.c_str(), stream) != LBM_OK ||
+            lbm_vtk_writer_submit(writer, LBM_VTK_SPEED, u, v, w, f_speed.c_str(), stream) != LBM_OK ||
+            lbm_vtk_writer_submit(writer, LBM_VTK_VECTOR, u, v, w, f_vel.c_str(), stream) != LBM_OK)
+            std::fprintf(stderr, "[vtk] %s\n", lbm_last_error());
     };
     if (vtk) {
         std::printf("[vtk] %s: dir=%s every=%d\n", tag, dir.string().c_str(), s.vtk_every);
@@ -280,7 +287,10 @@ inline int run(const Settings& s, int method, const char* tag) {
         if (vtk && step % s.vtk_every == 0) dump(step);
     }
     if (lbm_synchronize(h) != LBM_OK) return fail("step");
-    if (speed) cudaFree(speed);
+    if (writer) {
+        if (lbm_vtk_writer_flush(writer) != LBM_OK) std::fprintf(stderr, "[vtk] %s\n", lbm_last_error());
+        lbm_vtk_writer_destroy(writer);
+    }
     lbm_destroy(h);
     return 0;
 }

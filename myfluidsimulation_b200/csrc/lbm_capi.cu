@@ -605,6 +605,12 @@ int lbm_set_home_zchunk(lbm_solver* s, int zchunk) {
     return LBM_OK;
 }
 
+int lbm_solver_stream(lbm_solver* s, void** stream) {
+    if (!s || !stream) { set_error("lbm_solver_stream: null argument"); return LBM_ERR_INVALID; }
+    *stream = s->stream;
+    return LBM_OK;
+}
+
 int lbm_home_zchunk(lbm_solver* s, int* zchunk) {
     if (!s || !zchunk) { set_error("lbm_home_zchunk: null argument"); return LBM_ERR_INVALID; }
     *zchunk = s->home_zchunk;

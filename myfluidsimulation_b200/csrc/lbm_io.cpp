@@ -19,6 +19,7 @@
 
 namespace lbm {
 void set_error(const std::string& msg);
+int write_vtk_file(int kind, const float* a, const float* b, const float* c, int nx, int ny, int nz, const char* path);
 }
 
 namespace {
@@ -84,15 +85,6 @@ std::string read_all(const char* path, bool& ok) {
     return ss.str();
 }
 
-int vtk_header(std::ofstream& f, const char* kind, int Nx, int Ny, int Nz, size_t N) {
-    f << "# vtk DataFile Version 3.0\n" << kind << "\nASCII\n"
-      << "DATASET STRUCTURED_POINTS\n"
-      << "DIMENSIONS " << Nx << " " << Ny << " " << Nz << "\n"
-      << "ORIGIN 0 0 0\n"
-      << "SPACING 1 1 1\n"
-      << "POINT_DATA " << N << "\n";
-    return 0;
-}
 
 }  // namespace
 
@@ -122,38 +114,17 @@ int lbm_load_stl(const char* path, float** tris, int64_t* ntri, float* bb) {
 
 void lbm_free(void* p) { std::free(p); }
 
+// The text is formatted on the GPU (lbm_vtk.cu), byte-identical to the
+// reference's `ofstream << float` writer (src/moment_vtk_writer.cu:8-48).
 int lbm_write_scalar_vtk(const char* filename, const float* d_field, int Nx, int Ny, int Nz) {
-    const size_t N = (size_t)Nx * (size_t)Ny * (size_t)Nz;
-    std::vector<float> h(N);
-    if (cudaMemcpy(h.data(), d_field, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
-        lbm::set_error("write_scalar_vtk: device copy failed");
-        return LBM_ERR_CUDA;
-    }
-    std::ofstream f(filename);
-    if (!f) { lbm::set_error(std::string("failed to open VTK file: ") + filename); return LBM_ERR_IO; }
-    vtk_header(f, "scalar", Nx, Ny, Nz, N);
-    f << "SCALARS s float 1\n"
-      << "LOOKUP_TABLE default\n";
-    for (size_t i = 0; i < N; ++i) f << h[i] << "\n";
-    return f.good() ? LBM_OK : LBM_ERR_IO;
+    if (!filename || !d_field) { lbm::set_error("write_scalar_vtk: null argument"); return LBM_ERR_INVALID; }
+    return lbm::write_vtk_file(LBM_VTK_SCALAR, d_field, nullptr, nullptr, Nx, Ny, Nz, filename);
 }
 
 int lbm_write_vector_vtk(const char* filename, const float* d_fx, const float* d_fy, const float* d_fz, int Nx,
                          int Ny, int Nz) {
-    const size_t N = (size_t)Nx * (size_t)Ny * (size_t)Nz;
-    std::vector<float> h(3 * N);
-    if (cudaMemcpy(h.data(), d_fx, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(h.data() + N, d_fy, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(h.data() + 2 * N, d_fz, N * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) {
-        lbm::set_error("write_vector_vtk: device copy failed");
-        return LBM_ERR_CUDA;
-    }
-    std::ofstream f(filename);
-    if (!f) { lbm::set_error(std::string("failed to open VTK file: ") + filename); return LBM_ERR_IO; }
-    vtk_header(f, "vector", Nx, Ny, Nz, N);
-    f << "VECTORS vec float\n";
-    for (size_t i = 0; i < N; ++i) f << h[i] << " " << h[i + N] << " " << h[i + 2 * N] << "\n";
-    return f.good() ? LBM_OK : LBM_ERR_IO;
+    if (!filename || !d_fx || !d_fy || !d_fz) { lbm::set_error("write_vector_vtk: null argument"); return LBM_ERR_INVALID; }
+    return lbm::write_vtk_file(LBM_VTK_VECTOR, d_fx, d_fy, d_fz, Nx, Ny, Nz, filename);
 }
 
 void write_scalar_vtk(const char* filename, const float* d_field, int Nx, int Ny, int Nz) {

@@ -159,6 +159,13 @@ class Solver:
         return v.value
 
     # -- outputs -----------------------------------------------------------------
+    @property
+    def stream(self) -> int:
+        """The cudaStream_t this solver runs on."""
+        p = C.c_void_p()
+        check(lib().lbm_solver_stream(self._h, C.byref(p)))
+        return p.value or 0
+
     def macro_ptrs(self):
         p = [C.c_void_p() for _ in range(4)]
         check(lib().lbm_macro_ptrs(self._h, *[C.byref(x) for x in p]))

@@ -674,6 +674,76 @@ def vtk_study(args, torch):
     print(json.dumps(out))
 
 
+def render_study(args, torch):
+    """The viewer's volume view of the bench duct (256x128x128, Legacy after
+    200 steps) at 1280x720 with the viewer's default orbit camera and uStep
+    0.005 (main_compare.cpp:999), in its two displays: |u| with uScale 150
+    (opaque within a few samples) and rho-1 with uScale 1000 (mostly below the
+    0.15 threshold: long rays).  Frame time of the exact and texture-unit
+    samplers (CUDA events, median of 20), samples per second (the sample count
+    from the oracle, which marches the same rays), and the oracle itself on
+    the host cores as the baseline leg (one frame)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_bind import Oracle
+    from myfluidsimulation_b200 import lib
+    from myfluidsimulation_b200.render import FILTER_EXACT, FILTER_TEXTURE, VolumeRenderer, orbit_camera
+    st = torch.cuda.current_stream()
+    with tempfile.TemporaryDirectory() as td:
+        mask, _, _ = build_mask(td)
+    s, _ = make_solver("legacy", mask, st.cuda_stream)
+    s.step(200)
+    r, u, v, w = s.macro_ptrs()
+    N = NX * NY * NZ
+    speed = torch.empty(N, device="cuda")
+    torch.cuda.synchronize()
+    lib().launch_speed(u, v, w, speed.data_ptr(), N)
+    torch.cuda.synchronize()
+    W_, H_ = 1280, 720
+    inv, cam = orbit_camera(0.0, 0.3, 2.5, (0.5, 0.5, 0.5), W_, H_)
+    pres = torch.empty(N, device="cuda")
+    lib().launch_shift(r, -1.0, pres.data_ptr(), N)
+    torch.cuda.synchronize()
+    out = {"study": "render", "workload": f"duct {NX}x{NY}x{NZ} (Legacy, 200 steps), {W_}x{H_}, orbit yaw 0 "
+                                          "pitch 0.3 radius 2.5, uStep 0.005, uThresh 0.15"}
+    orc = Oracle()
+    with VolumeRenderer(NX, NY, NZ) as rr:
+        img = None
+        for view, field, scale in (("speed", speed, 150.0), ("pressure", pres, 1000.0)):
+            host = field.cpu().numpy().reshape(NZ, NY, NX)
+            t0 = time.perf_counter()
+            ref_img, samples = orc.raymarch(host, inv, cam, 0.005, scale, 0.15, W_, H_)
+            dt = time.perf_counter() - t0
+            res_v = {"uScale": scale, "samples_per_frame": samples,
+                     "cpu_baseline": {"value": round(dt * 1e3, 1), "unit": "ms per frame",
+                                      "cores": orc.lib.orc_num_threads(), "kind": "port",
+                                      "sample": "one frame, the oracle's FP32 restatement of the shader"}}
+            for name, flt in (("exact", FILTER_EXACT), ("texture", FILTER_TEXTURE)):
+                ts = []
+                for it in range(25):
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(st)
+                    img = rr.render(field, inv, cam, W_, H_, 0.005, scale, 0.15, flt, out=img)
+                    e1.record(st)
+                    torch.cuda.synchronize()
+                    if it >= 5:
+                        ts.append(e0.elapsed_time(e1))
+                ms = statistics.median(ts)
+                res = {"ms_per_frame": round(ms, 3), "fps": round(1e3 / ms, 1),
+                       "gsamples_per_s": round(samples / ms / 1e6, 2)}
+                got = img.cpu().numpy()
+                if flt == FILTER_EXACT:
+                    res["bit_identical_to_oracle"] = bool(np.array_equal(got, ref_img))
+                else:
+                    d = np.abs(np.clip(got[..., :3], 0, 1) - np.clip(ref_img[..., :3], 0, 1)).max(axis=2)
+                    res["displayed_mean_abs_diff_vs_oracle"] = float(d.mean())
+                res["speedup_vs_cpu_baseline"] = round(dt * 1e3 / ms, 1)
+                res_v[name] = res
+            out[view] = res_v
+    s.close()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -684,11 +754,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default=None,
                     help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
-    ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint", "vtk"],
+    ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint", "vtk", "render"],
                     help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage; "
                          "batch: 64 uneven Hybrid(B0) ducts in one persistent launch per step; "
                          "adjoint: drag gradient of the 128x64x64 duct against central differences; "
-                         "vtk: snapshot cost of the GPU VTK writers against the reference's writer")
+                         "vtk: snapshot cost of the GPU VTK writers against the reference's writer; "
+                         "render: the viewer's volume ray-march of the duct's |u| at 1280x720")
     ap.add_argument("--vtk-steps", type=int, default=1000)
     ap.add_argument("--vtk-every", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
@@ -730,6 +801,9 @@ def main():
         return
     if args.study == "vtk":
         vtk_study(args, torch)
+        return
+    if args.study == "render":
+        render_study(args, torch)
         return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)

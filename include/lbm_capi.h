@@ -377,6 +377,43 @@ int lbm_format_g6(const float* v, int64_t n, char* out, int32_t stride, uint8_t*
 /* The CUDA stream a solver runs on (cudaStream_t). */
 int lbm_solver_stream(lbm_solver* s, void** stream);
 
+/* ---- headless volume view ------------------------------------------------ */
+
+/* The viewer's other field helpers, same names and signatures
+ * (src/fields/field_ops.cu:29-41): out = a - b, out = a + bias. */
+void launch_diff(const float* a, const float* b, float* out, int N);
+void launch_shift(const float* a, float bias, float* out, int N);
+
+/* Samplers of lbm_render_volume: trilinear in FP32 exactly as written
+ * (reproducible, equal to the C oracle), or the texture unit's filter. */
+enum { LBM_FILTER_EXACT = 0, LBM_FILTER_TEXTURE = 1 };
+/* Uniforms of the reference's volume shader (src/render/Vis3D.cpp:30-78,
+ * set at Vis3D.cpp:128-138). */
+typedef struct lbm_render_params {
+    int32_t width, height;   /* framebuffer (main_compare: 1280 x 720) */
+    float inv_pv[16];        /* inverse(P V), column-major */
+    float cam_pos[3];
+    float step;              /* uStep (0.005 in main_compare.cpp:999) */
+    float scale;             /* uScale (150 speed, 1000 rho-1, 2000 difference) */
+    float threshold;         /* uThresh (0.15) */
+    int32_t filter;          /* LBM_FILTER_* */
+} lbm_render_params;
+/* Ray-marches the Nx*Ny*Nz device field (x fastest, mapped onto [0,1]^3) into
+ * d_rgba (width*height float RGBA, row 0 at the bottom) on `stream`.  Replaces
+ * Vis3D::uploadScalar + renderVolume (Vis3D.cpp:118-138) without the host
+ * round trip and the GL context. */
+typedef struct lbm_renderer lbm_renderer;
+int lbm_renderer_create(int32_t nx, int32_t ny, int32_t nz, lbm_renderer** out);
+int lbm_render_volume(lbm_renderer* r, const float* d_field, const lbm_render_params* p, float* d_rgba,
+                      void* stream);
+int lbm_renderer_destroy(lbm_renderer* r);
+/* The viewer's orbit camera (main_compare.cpp:51-60,972-981): inverse(P V)
+ * and the eye position for yaw/pitch/radius around target. */
+int lbm_render_orbit_camera(float yaw, float pitch, float radius, const float* target, int32_t width,
+                            int32_t height, float* inv_pv, float* cam_pos);
+/* Host RGBA float image -> binary PPM, top row first, 8 bits per channel. */
+int lbm_write_ppm(const char* path, const float* rgba, int32_t width, int32_t height);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

@@ -20,6 +20,7 @@ ERRORS = {1: "LBM_ERR_INVALID", 2: "LBM_ERR_CUDA", 3: "LBM_ERR_ALLOC", 4: "LBM_E
 METHOD_LEGACY, METHOD_HOME, METHOD_HYBRID = 0, 1, 2
 STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
 VTK_SCALAR, VTK_SPEED, VTK_VECTOR = 0, 1, 2
+FILTER_EXACT, FILTER_TEXTURE = 0, 1
 BC_PERIODIC, BC_DUCT = 0, 1
 BOUNCE_HALFWAY, BOUNCE_REFERENCE = 0, 1
 NSTAT = 8
@@ -58,6 +59,11 @@ class AdjProblem(C.Structure):
 
 
 # (name, restype, argtypes)
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("inv_pv", C.c_float * 16), ("cam_pos", C.c_float * 3),
+                ("step", C.c_float), ("scale", C.c_float), ("threshold", C.c_float), ("filter", C.c_int32)]
+
+
 _P = C.c_void_p
 _PROTOS = [
     ("lbm_last_error", C.c_char_p, []),
@@ -124,6 +130,13 @@ _PROTOS = [
     ("lbm_vtk_writer_destroy", C.c_int, [_P]),
     ("lbm_format_g6", C.c_int, [_P, C.c_int64, _P, C.c_int32, _P]),
     ("lbm_solver_stream", C.c_int, [_P, C.POINTER(_P)]),
+    ("launch_diff", None, [_P, _P, _P, C.c_int]),
+    ("launch_shift", None, [_P, C.c_float, _P, C.c_int]),
+    ("lbm_renderer_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P)]),
+    ("lbm_render_volume", C.c_int, [_P, _P, C.POINTER(RenderParams), _P, _P]),
+    ("lbm_renderer_destroy", C.c_int, [_P]),
+    ("lbm_render_orbit_camera", C.c_int, [C.c_float, C.c_float, C.c_float, _P, C.c_int32, C.c_int32, _P, _P]),
+    ("lbm_write_ppm", C.c_int, [C.c_char_p, _P, C.c_int32, C.c_int32]),
 ]
 
 EXPORTED = [n for n, _, _ in _PROTOS]

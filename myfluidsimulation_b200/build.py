@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
            "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]
 
-SOURCES = ["lbm_aa.cu", "lbm_push.cu", "lbm_home.cu", "lbm_aux.cu", "lbm_geom.cu", "lbm_capi.cu", "lbm_static.cu", "lbm_adjoint.cu", "lbm_vtk.cu", "lbm_io.cpp"]
+SOURCES = ["lbm_aa.cu", "lbm_push.cu", "lbm_home.cu", "lbm_aux.cu", "lbm_geom.cu", "lbm_capi.cu", "lbm_static.cu", "lbm_adjoint.cu", "lbm_vtk.cu", "lbm_render.cu", "lbm_io.cpp"]
 HEADERS = ["lbm_common.cuh", "lbm_internal.h"]
 APP_NAMES = ["fluidsim_legacy", "fluidsim_home", "fluidsim_hybrid", "fluidsim_tgv", "fluidsim_sweep"]
 

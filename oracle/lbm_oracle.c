@@ -6,7 +6,11 @@
  *   - D3Q19 LBM steps in FP64 (and an FP32 twin), lbm_oracle_impl.h;
  *   - the B0 band classification, src/apps/sim_runner.hpp:28-91;
  *   - the STL loader, src/geom/stl_loader.cpp:34-122;
- *   - the SAT + flood-fill voxelizer, src/geom/voxelize.cpp:14-243.
+ *   - the SAT + flood-fill voxelizer, src/geom/voxelize.cpp:14-243;
+ *   - the volume view's fragment shader (src/render/Vis3D.cpp:30-78), in FP32
+ *     with every operation rounded as written.  That one is parity unpinned:
+ *     the shader needs an OpenGL context, unavailable on this box, so it is
+ *     restated from its GLSL source alone.
  * The geometry code computes in float with no contraction (built with
  * -ffp-contract=off), in the reference's operation order, so that masks are
  * bit-exact with the reference compiled by a default x86-64 g++.
@@ -355,4 +359,112 @@ int orc_voxelize(const float* tris, int64_t ntri, const float* bb, int nx, int n
     }
     free(surf); free(vt);
     return 0;
+}
+
+/* ---- volume view: the fragment shader of src/render/Vis3D.cpp:30-78 ------ */
+
+/* GLSL min/max/clamp/mix as the specification writes them */
+static float g_min(float x, float y) { return y < x ? y : x; }
+static float g_max(float x, float y) { return x < y ? y : x; }
+static float g_clamp(float x, float lo, float hi) { return g_min(g_max(x, lo), hi); }
+static float g_mix(float x, float y, float a) { return x * (1.0f - a) + y * a; }
+
+/* colormap(t), Vis3D.cpp:40-46 */
+static void vs_colormap(float t, float c[3]) {
+    static const float K[5][3] = {{0.02f, 0.02f, 0.2f}, {0.0f, 0.7f, 1.0f}, {0.0f, 1.0f, 0.3f},
+                                  {1.0f, 0.9f, 0.0f}, {1.0f, 0.1f, 0.0f}};
+    t = g_clamp(t, 0.0f, 1.0f);
+    int seg;
+    float w;
+    if (t < 0.25f) { seg = 0; w = t * 4.0f; }
+    else if (t < 0.50f) { seg = 1; w = (t - 0.25f) * 4.0f; }
+    else if (t < 0.75f) { seg = 2; w = (t - 0.50f) * 4.0f; }
+    else { seg = 3; w = (t - 0.75f) * 4.0f; }
+    for (int k = 0; k < 3; ++k) c[k] = g_mix(K[seg][k], K[seg + 1][k], w);
+}
+
+/* texture(uTex, p).r with GL_LINEAR and CLAMP_TO_EDGE on an R32F 3-D texture
+ * (Vis3D.cpp:82-89): texel i centred at (i + 0.5) / n, lerp in x, y, z */
+static float vs_texture(const float* f, int nx, int ny, int nz, const float p[3]) {
+    const int n[3] = {nx, ny, nz};
+    int i0[3], i1[3];
+    float fr[3];
+    for (int k = 0; k < 3; ++k) {
+        const float u = p[k] * (float)n[k] - 0.5f;
+        const float fl = floorf(u);
+        const int i = (int)fl;
+        fr[k] = u - fl;
+        i0[k] = i < 0 ? 0 : (i > n[k] - 1 ? n[k] - 1 : i);
+        i1[k] = i + 1 < 0 ? 0 : (i + 1 > n[k] - 1 ? n[k] - 1 : i + 1);
+    }
+#define TX(x, y, z) f[((size_t)(z) * ny + (y)) * nx + (x)]
+    const float c00 = g_mix(TX(i0[0], i0[1], i0[2]), TX(i1[0], i0[1], i0[2]), fr[0]);
+    const float c10 = g_mix(TX(i0[0], i1[1], i0[2]), TX(i1[0], i1[1], i0[2]), fr[0]);
+    const float c01 = g_mix(TX(i0[0], i0[1], i1[2]), TX(i1[0], i0[1], i1[2]), fr[0]);
+    const float c11 = g_mix(TX(i0[0], i1[1], i1[2]), TX(i1[0], i1[1], i1[2]), fr[0]);
+#undef TX
+    return g_mix(g_mix(c00, c10, fr[1]), g_mix(c01, c11, fr[1]), fr[2]);
+}
+
+/* One frame: main() of the shader for every pixel (x, y), uv = ((x+0.5)/W,
+ * (y+0.5)/H), row 0 at the bottom; a discarded fragment keeps the clear colour
+ * (0.02, 0.02, 0.03, 1) of main_compare.cpp:988.  inv_pv column-major. */
+void orc_raymarch_f32(const float* field, int nx, int ny, int nz, const float* inv_pv, const float* cam,
+                      float step, float scale, float thresh, int width, int height, float* rgba,
+                      int64_t* samples) {
+    int64_t total = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+:total)
+    for (int y = 0; y < height; ++y) {
+        for (int x = 0; x < width; ++x) {
+            float* o = rgba + ((size_t)y * width + x) * 4;
+            const float uvx = ((float)x + 0.5f) / (float)width, uvy = ((float)y + 0.5f) / (float)height;
+            const float ndc[4] = {uvx * 2.0f - 1.0f, uvy * 2.0f - 1.0f, 0.0f, 1.0f};
+            float w[4];
+            for (int r = 0; r < 4; ++r)
+                w[r] = inv_pv[r] * ndc[0] + inv_pv[4 + r] * ndc[1] + inv_pv[8 + r] * ndc[2] + inv_pv[12 + r] * ndc[3];
+            float dir[3];
+            for (int k = 0; k < 3; ++k) dir[k] = w[k] / w[3] - cam[k];
+            const float len = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+            for (int k = 0; k < 3; ++k) dir[k] = dir[k] / len;
+            float t0[3], t1[3];
+            for (int k = 0; k < 3; ++k) {
+                t0[k] = (0.0f - cam[k]) / dir[k];
+                t1[k] = (1.0f - cam[k]) / dir[k];
+            }
+            float tnear = g_max(g_max(g_min(t0[0], t1[0]), g_min(t0[1], t1[1])), g_min(t0[2], t1[2]));
+            const float tfar = g_min(g_min(g_max(t0[0], t1[0]), g_max(t0[1], t1[1])), g_max(t0[2], t1[2]));
+            if (tfar < 0.0f || tnear > tfar) {
+                o[0] = 0.02f; o[1] = 0.02f; o[2] = 0.03f; o[3] = 1.0f;
+                continue;
+            }
+            tnear = g_max(tnear, 0.0f);
+            float pos[3];
+            for (int k = 0; k < 3; ++k) pos[k] = cam[k] + dir[k] * tnear;
+            float t = tnear, acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            while (t < tfar && acc[3] < 0.95f) {
+                /* sampleVol(pos), Vis3D.cpp:48-57 */
+                const float s = vs_texture(field, nx, ny, nz, pos) * scale;
+                const float tmag = g_clamp(fabsf(s), 0.0f, 1.0f);
+                float sr = 0.0f, sg = 0.0f, sb = 0.0f, sa = 0.0f;
+                if (!(tmag < thresh)) {
+                    const float tcol = 0.5f + 0.5f * g_clamp(s, -1.0f, 1.0f);
+                    const float h = g_clamp((tmag - thresh) / (1.0f - thresh), 0.0f, 1.0f);   /* smoothstep */
+                    float c[3];
+                    vs_colormap(tcol, c);
+                    sr = c[0]; sg = c[1]; sb = c[2];
+                    sa = h * h * (3.0f - 2.0f * h);
+                }
+                const float rem = 1.0f - acc[3];
+                acc[0] += sr * rem;
+                acc[1] += sg * rem;
+                acc[2] += sb * rem;
+                acc[3] += sa * (1.0f - acc[3]);
+                for (int k = 0; k < 3; ++k) pos[k] += dir[k] * step;
+                t += step;
+                ++total;
+            }
+            o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2]; o[3] = 1.0f;
+        }
+    }
+    if (samples) *samples = total;
 }

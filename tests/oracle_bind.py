@@ -96,6 +96,20 @@ class Oracle:
             _p(drag))
         return a, drag
 
+    # -- volume view -----------------------------------------------------------
+    def raymarch(self, field, inv_pv, cam, step, scale, thresh, width, height):
+        """The shader of src/render/Vis3D.cpp:30-78 on the CPU -> (rgba[h, w, 4], samples)."""
+        f = np.ascontiguousarray(field, np.float32)
+        nz, ny, nx = f.shape
+        m = np.ascontiguousarray(inv_pv, np.float32).ravel()
+        c = np.ascontiguousarray(cam, np.float32).ravel()
+        out = np.empty((height, width, 4), np.float32)
+        ns = C.c_int64()
+        self.lib.orc_raymarch_f32(_p(f), C.c_int(nx), C.c_int(ny), C.c_int(nz), _p(m), _p(c), C.c_float(step),
+                                  C.c_float(scale), C.c_float(thresh), C.c_int(width), C.c_int(height), _p(out),
+                                  C.byref(ns))
+        return out, ns.value
+
     # -- geometry ------------------------------------------------------------
     def band(self, mask, d0):
         m = np.ascontiguousarray(mask, np.uint8)

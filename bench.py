@@ -744,6 +744,70 @@ def render_study(args, torch):
     print(json.dumps(out))
 
 
+def slab_study(args, torch):
+    """The bench duct (256x128x128, Legacy, FP32) split into z-slabs on this one
+    GPU: the single-device image of the multi-GPU decomposition.  Per slab count:
+    MLUPS over 200 steps (CUDA events) against the single grid, the bytes that
+    cross the slab faces per step pair (the 5 slot planes of each face, out in
+    phase 0 and back in phase 1), and the time those bytes would take over
+    NVLink at the measured 770 GB/s per direction between two GPUs."""
+    from myfluidsimulation_b200.slabs import SlabSet
+    from myfluidsimulation_b200.solvers import BC_DUCT, METHOD_LEGACY, Solver
+    with tempfile.TemporaryDirectory() as td:
+        mask, _, _ = build_mask(td)
+    rho = np.ones((NZ, NY, NX), np.float32)
+    u = np.full((NZ, NY, NX), U_IN, np.float32)
+    u[mask != 0] = 0
+    st = torch.cuda.Stream()
+    N = NX * NY * NZ
+    steps = 200
+    out = {"study": "slab", "workload": f"duct {NX}x{NY}x{NZ} Legacy FP32, {steps} steps, z-slabs on one GPU, "
+                                        "every run replayed from a CUDA graph of 20 steps"}
+    base = None
+    for parts in (1, 2, 4, 8):
+        with torch.cuda.stream(st):
+            if parts == 1:
+                obj = Solver(NX, NY, NZ, TAU, method=METHOD_LEGACY, bc=BC_DUCT, inlet_u=U_IN,
+                             stream=st.cuda_stream)
+            else:
+                obj = SlabSet(NX, NY, NZ, TAU, parts, method=METHOD_LEGACY, bc=BC_DUCT, inlet_u=U_IN,
+                              stream=st.cuda_stream)
+            obj.set_solid_mask(mask)
+            obj.reinit_from_host(rho, u, None, None)
+            obj.set_macro_output(False)
+            obj.step(10)
+            torch.cuda.synchronize()
+            if parts == 1:
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=st):
+                    obj.step(20)
+            else:
+                g = obj.graph(20)
+            g.replay()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps // 20):
+                g.replay()
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            del g
+        mlups = N * steps / (ms * 1e-3) / 1e6
+        face = 5 * NX * NY * 4
+        r = {"mlups": round(mlups, 1), "us_per_step": round(ms * 1e3 / steps, 1)}
+        if parts == 1:
+            base = mlups
+        else:
+            # per odd step each face moves 5 slot planes each way (phase 0), and back (phase 1)
+            r["face_bytes_per_step_pair"] = 4 * face
+            r["nvlink_us_per_step_pair_at_770GBs"] = round(2 * face / 770e9 * 1e6 * 2, 1)
+            r["vs_single_grid"] = round(mlups / base, 3)
+        out[f"slabs_{parts}"] = r
+        obj.close()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -754,12 +818,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default=None,
                     help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
-    ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint", "vtk", "render"],
+    ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint", "vtk", "render", "slab"],
                     help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage; "
                          "batch: 64 uneven Hybrid(B0) ducts in one persistent launch per step; "
                          "adjoint: drag gradient of the 128x64x64 duct against central differences; "
                          "vtk: snapshot cost of the GPU VTK writers against the reference's writer; "
-                         "render: the viewer's volume ray-march of the duct's |u| at 1280x720")
+                         "render: the viewer's volume ray-march of the duct's |u| at 1280x720; "
+                         "slab: the duct split into z-slabs on one GPU (the multi-GPU decomposition)")
     ap.add_argument("--vtk-steps", type=int, default=1000)
     ap.add_argument("--vtk-every", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
@@ -804,6 +869,9 @@ def main():
         return
     if args.study == "render":
         render_study(args, torch)
+        return
+    if args.study == "slab":
+        slab_study(args, torch)
         return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)

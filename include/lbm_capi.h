@@ -376,6 +376,38 @@ int lbm_vtk_writer_destroy(lbm_vtk_writer* w);
 int lbm_format_g6(const float* v, int64_t n, char* out, int32_t stride, uint8_t* lens);
 /* The CUDA stream a solver runs on (cudaStream_t). */
 int lbm_solver_stream(lbm_solver* s, void** stream);
+/* Parity of the next AA step (0: the local step, 1: the neighbour step). */
+int lbm_step_parity(lbm_solver* s, int* parity);
+
+/* ---- z-slab decomposition (Legacy/Hybrid, halfway bounce-back) ----------- */
+
+/* A slab solver of nz planes steps only planes 1..nz-2; planes 0 and nz-1 are
+ * ghost copies of the neighbouring slabs' boundary planes (give them the
+ * neighbours' mask, band and initial fields).  No reference counterpart: the
+ * reference runs one grid on one GPU. */
+int lbm_set_z_ghosts(lbm_solver* s, int on);
+/* Device addresses of the 5 slot planes of `plane` whose direction has
+ * c_z = cz (+1 or -1), in direction order, each *bytes long: what crosses a
+ * slab face in an odd step. */
+int lbm_zslab_slots(lbm_solver* s, int plane, int cz, void** ptrs, int64_t* bytes);
+/* Exchange between two slabs on this device, `lower` below `upper` (periodic
+ * wrap: the top slab is `lower` of the bottom one).  Before each odd step
+ * (parity 1) call phase 0 on every face: boundary slots -> neighbour's ghost;
+ * after it phase 1: ghost slots -> their owner's boundary plane. */
+int lbm_zslab_exchange(lbm_solver* lower, lbm_solver* upper, int phase, void* stream);
+/* Phase 1 for slabs on different devices: after receiving a neighbour's ghost
+ * slot planes (5 device buffers, direction order) for `plane` / `cz`, take the
+ * values its cells wrote: every cell whose link towards that neighbour
+ * streams (a cell that bounced its own population back keeps it). */
+int lbm_zslab_merge(lbm_solver* s, int plane, int cz, void* const* src, void* stream);
+/* Every face of a periodic chain of n slabs (slab k below slab k+1, the last
+ * below the first) in ONE launch per phase: the transfers of lbm_zslab_exchange
+ * for all faces, as a job table built once.  The slabs' buffers must stay in
+ * place (no re-creation) while the plan lives.  Capturable in CUDA graphs. */
+typedef struct lbm_zslab_plan lbm_zslab_plan;
+int lbm_zslab_plan_create(lbm_solver* const* slabs, int32_t n, lbm_zslab_plan** out);
+int lbm_zslab_plan_exchange(lbm_zslab_plan* p, int phase, void* stream);
+int lbm_zslab_plan_destroy(lbm_zslab_plan* p);
 
 /* ---- headless volume view ------------------------------------------------ */
 

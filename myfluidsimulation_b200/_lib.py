@@ -130,6 +130,14 @@ _PROTOS = [
     ("lbm_vtk_writer_destroy", C.c_int, [_P]),
     ("lbm_format_g6", C.c_int, [_P, C.c_int64, _P, C.c_int32, _P]),
     ("lbm_solver_stream", C.c_int, [_P, C.POINTER(_P)]),
+    ("lbm_step_parity", C.c_int, [_P, C.POINTER(C.c_int)]),
+    ("lbm_set_z_ghosts", C.c_int, [_P, C.c_int]),
+    ("lbm_zslab_slots", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P), C.POINTER(C.c_int64)]),
+    ("lbm_zslab_exchange", C.c_int, [_P, _P, C.c_int, _P]),
+    ("lbm_zslab_merge", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P), _P]),
+    ("lbm_zslab_plan_create", C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
+    ("lbm_zslab_plan_exchange", C.c_int, [_P, C.c_int, _P]),
+    ("lbm_zslab_plan_destroy", C.c_int, [_P]),
     ("launch_diff", None, [_P, _P, _P, C.c_int]),
     ("launch_shift", None, [_P, C.c_float, _P, C.c_int]),
     ("lbm_renderer_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(_P)]),

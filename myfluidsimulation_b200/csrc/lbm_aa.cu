@@ -192,11 +192,11 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
 template <class ST, bool MASK, int VEC, int MODE, class IDX>
 __global__ void __launch_bounds__(256, 2) aa_even(AAParams p) {
     constexpr bool STATS = MODE == 2;
-    const IDX nvec = (IDX)p.N / VEC;
+    const IDX v0 = (IDX)(p.first / VEC), v1 = (IDX)((p.first + p.cells) / VEC);
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-    for (IDX v = (IDX)blockIdx.x * blockDim.x + threadIdx.x; v < nvec; v += (IDX)gridDim.x * blockDim.x)
+    for (IDX v = v0 + (IDX)blockIdx.x * blockDim.x + threadIdx.x; v < v1; v += (IDX)gridDim.x * blockDim.x)
         even_unit<ST, MASK, VEC, MODE, IDX>(p, v, acc);
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }
@@ -288,13 +288,14 @@ __global__ void __launch_bounds__(256, MASK ? 4 : 3) aa_odd(AAParams p) {
     constexpr bool STATS = MODE == 2;
     const int bx = blockDim.x;
     const int segs = (p.nx + bx - 1) / bx;
-    const IDX total = (IDX)segs * p.ny * p.nz;
+    const IDX row0 = (IDX)(p.first / p.nx);
+    const IDX total = (IDX)segs * (IDX)(p.cells / p.nx);
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
     for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
-        const IDX row = sg / segs;
-        const int x = (int)(sg - row * segs) * bx + threadIdx.x;
+        const IDX row = row0 + sg / segs;
+        const int x = (int)(sg - (sg / segs) * segs) * bx + threadIdx.x;
         if (x < p.nx) odd_cell<ST, MASK, MODE, IDX>(p, row, x, acc);
     }
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
@@ -334,10 +335,11 @@ void launch_mode(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
     // consecutive cells per thread: two in FP32 (8-byte accesses), four in F16/BF16 (8-byte accesses)
     constexpr int V = ST::kId == 0 ? 2 : 4;
     if (parity == 0) {
-        if (V == 4 && p.N % 4 != 0 && p.N % 2 == 0) {
+        const int64_t span = p.first | p.cells;      // both must be multiples of the vector width
+        if (V == 4 && span % 4 != 0 && span % 2 == 0) {
             if (mask) aa_even<ST, true, 2, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
             else aa_even<ST, false, 2, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
-        } else if (p.N % V == 0) {
+        } else if (span % V == 0) {
             if (mask) aa_even<ST, true, V, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
             else aa_even<ST, false, V, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
         } else {

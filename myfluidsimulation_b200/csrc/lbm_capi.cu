@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "lbm_capi.h"
+#include "lbm_common.cuh"
 #include "lbm_internal.h"
 
 namespace lbm {
@@ -63,6 +64,7 @@ struct lbm_solver {
     int64_t steps = 0;
     lbm::LaunchCfg cfg_even{0, 256}, cfg_odd{0, 256};
     int home_zchunk = 16;
+    bool zghost = false;        // z-slab: planes 0 and nz-1 are ghosts, steps cover 1..nz-2
     // graph cache
     cudaGraphExec_t gexec = nullptr;
     int g_sub = 0, g_parity = -1, g_stats = -1;
@@ -132,6 +134,9 @@ lbm::AAParams aa_params(lbm_solver* s, bool macro, bool stats) {
     p.macro = macro;
     p.partials = s->partials;
     p.stats = stats;
+    const int64_t plane = (int64_t)s->dom.nx * s->dom.ny;
+    p.first = s->zghost ? plane : 0;
+    p.cells = s->zghost ? s->N - 2 * plane : s->N;
     return p;
 }
 
@@ -201,6 +206,68 @@ static int enqueue_steps(lbm_solver* s, int n) {
         CK(lbm::launch_home_macros(s->m[s->cur], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
                                    s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
     s->steps += n;
+    return LBM_OK;
+}
+
+namespace {
+// Phase 1 writes back only what the neighbour's cells wrote: slot q of a
+// boundary cell c is written by the cell c - c_q when the link between them
+// streams, and by c itself (bounce-back, inlet, outlet) when c's link in
+// direction opp(q) does not; a solid c is never written.
+template <class T>
+__global__ void zslab_merge(T* __restrict__ dst, const T* __restrict__ src, const uint8_t* __restrict__ flags,
+                            const uint32_t* __restrict__ links, int64_t n, int back_bit) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (flags && ((flags[i] & lbm::F_SOLID) || ((links[i] >> back_bit) & 1u))) continue;
+        dst[i] = src[i];
+    }
+}
+}  // namespace
+
+// One launch for every face of a chain of slabs: job j copies (or, with
+// flags, merges) one slot plane.  blockIdx.y is the job.
+struct SlabJob {
+    void* dst;
+    const void* src;
+    const uint8_t* flags;     // null: plain copy
+    const uint32_t* links;
+    int64_t n;                // elements
+    int back_bit;
+    int pad;
+};
+
+template <class T>
+__global__ void zslab_jobs(const SlabJob* __restrict__ jobs) {
+    const SlabJob j = jobs[blockIdx.y];
+    T* __restrict__ dst = static_cast<T*>(j.dst);
+    const T* __restrict__ src = static_cast<const T*>(j.src);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < j.n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (j.flags && ((j.flags[i] & lbm::F_SOLID) || ((j.links[i] >> j.back_bit) & 1u))) continue;
+        dst[i] = src[i];
+    }
+}
+
+static int merge_slots(lbm_solver* s, int plane, int cz, void* const* src, cudaStream_t st) {
+    void* dst[5];
+    int64_t b = 0;
+    int rc = lbm_zslab_slots(s, plane, cz, dst, &b);
+    if (rc != LBM_OK) return rc;
+    const int64_t pl = (int64_t)s->dom.nx * s->dom.ny;
+    const uint8_t* fl = s->use_flags ? s->flags + plane * pl : nullptr;
+    const uint32_t* lk = s->links + plane * pl;
+    const int blocks = (int)std::min<int64_t>((pl + 255) / 256, 4096);
+    int k = 0;
+    for (int q = 0; q < 19; ++q) {
+        if (lbm::cz(q) != cz) continue;
+        if (s->esize == 4)
+            zslab_merge<uint32_t><<<blocks, 256, 0, st>>>(static_cast<uint32_t*>(dst[k]),
+                                                          static_cast<const uint32_t*>(src[k]), fl, lk, pl, lbm::opp(q));
+        else
+            zslab_merge<uint16_t><<<blocks, 256, 0, st>>>(static_cast<uint16_t*>(dst[k]),
+                                                          static_cast<const uint16_t*>(src[k]), fl, lk, pl, lbm::opp(q));
+        ++k;
+    }
+    CK(cudaGetLastError());
     return LBM_OK;
 }
 
@@ -605,6 +672,165 @@ int lbm_set_home_zchunk(lbm_solver* s, int zchunk) {
     return LBM_OK;
 }
 
+// ---- z-slab decomposition ---------------------------------------------------
+//
+// A slab solver holds its interior planes 1..nz-2 and one ghost plane at each
+// end.  The even AA step is local.  In the odd step the slots of plane k with
+// c_z = -1 are read and rewritten only by the cells of plane k+1, and those with
+// c_z = +1 only by the cells of plane k-1.  So around each odd step the 5 slot
+// planes that cross a slab face travel to the neighbour's ghost plane (phase 0)
+// and, after it, back into the owner's boundary plane (phase 1).  Nothing else
+// is exchanged.
+
+
+int lbm_set_z_ghosts(lbm_solver* s, int on) {
+    if (!s) { set_error("lbm_set_z_ghosts: null solver"); return LBM_ERR_INVALID; }
+    if (!is_aa(s) || is_ref_push(s)) {
+        set_error("lbm_set_z_ghosts: Legacy/Hybrid with halfway bounce-back only");
+        return LBM_ERR_UNSUPPORTED;
+    }
+    if (on && s->dom.nz < 3) { set_error("lbm_set_z_ghosts: needs nz >= 3 (two ghost planes)"); return LBM_ERR_INVALID; }
+    s->zghost = on != 0;
+    drop_graph(s);
+    return LBM_OK;
+}
+
+int lbm_zslab_slots(lbm_solver* s, int plane, int cz, void** ptrs, int64_t* bytes) {
+    if (!s || !ptrs || !bytes || (cz != 1 && cz != -1) || plane < 0 || plane >= s->dom.nz) {
+        set_error("lbm_zslab_slots: bad argument");
+        return LBM_ERR_INVALID;
+    }
+    if (!is_aa(s) || is_ref_push(s)) { set_error("lbm_zslab_slots: AA solvers only"); return LBM_ERR_UNSUPPORTED; }
+    const int64_t pl = (int64_t)s->dom.nx * s->dom.ny;
+    char* base = static_cast<char*>(s->f);
+    int k = 0;
+    for (int q = 0; q < 19; ++q)     // the 5 directions with c_z = cz, in index order
+        if (lbm::cz(q) == cz) ptrs[k++] = base + s->esize * ((int64_t)q * s->N + (int64_t)plane * pl);
+    *bytes = (int64_t)s->esize * pl;
+    return LBM_OK;
+}
+
+int lbm_zslab_exchange(lbm_solver* lower, lbm_solver* upper, int phase, void* stream) {
+    if (!lower || !upper || (phase != 0 && phase != 1)) { set_error("lbm_zslab_exchange: bad argument"); return LBM_ERR_INVALID; }
+    if (!lower->zghost || !upper->zghost || lower->dom.nx != upper->dom.nx || lower->dom.ny != upper->dom.ny ||
+        lower->storage != upper->storage) {
+        set_error("lbm_zslab_exchange: needs two z-slab solvers of the same x-y size and storage");
+        return LBM_ERR_INVALID;
+    }
+    void *lo_top[5], *lo_ghost[5], *up_ghost[5], *up_bot[5];
+    int64_t b = 0;
+    int rc;
+    if ((rc = lbm_zslab_slots(lower, lower->dom.nz - 2, -1, lo_top, &b)) != LBM_OK ||
+        (rc = lbm_zslab_slots(lower, lower->dom.nz - 1, 1, lo_ghost, &b)) != LBM_OK ||
+        (rc = lbm_zslab_slots(upper, 0, -1, up_ghost, &b)) != LBM_OK ||
+        (rc = lbm_zslab_slots(upper, 1, 1, up_bot, &b)) != LBM_OK)
+        return rc;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (phase == 0) {   // boundary planes -> the neighbour's ghosts
+        for (int k = 0; k < 5; ++k) {
+            CK(cudaMemcpyAsync(up_ghost[k], lo_top[k], (size_t)b, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(lo_ghost[k], up_bot[k], (size_t)b, cudaMemcpyDeviceToDevice, st));
+        }
+        return LBM_OK;
+    }
+    // what the odd step streamed into the ghosts -> their owners
+    if ((rc = merge_slots(lower, lower->dom.nz - 2, -1, up_ghost, st)) != LBM_OK) return rc;
+    return merge_slots(upper, 1, 1, lo_ghost, st);
+}
+
+int lbm_zslab_merge(lbm_solver* s, int plane, int cz, void* const* src, void* stream) {
+    if (!s || !src || (cz != 1 && cz != -1)) { set_error("lbm_zslab_merge: bad argument"); return LBM_ERR_INVALID; }
+    if (!s->zghost) { set_error("lbm_zslab_merge: not a z-slab solver"); return LBM_ERR_INVALID; }
+    return merge_slots(s, plane, cz, src, static_cast<cudaStream_t>(stream));
+}
+
+struct lbm_zslab_plan {
+    SlabJob* d_jobs[2] = {nullptr, nullptr};   // phase 0 copies, phase 1 merges
+    int njobs = 0;
+    int esize = 4;
+    int64_t elems = 0;
+};
+
+int lbm_zslab_plan_create(lbm_solver* const* slabs, int32_t n, lbm_zslab_plan** out) {
+    if (!slabs || n < 1 || !out) { set_error("lbm_zslab_plan_create: bad argument"); return LBM_ERR_INVALID; }
+    for (int k = 0; k < n; ++k) {
+        const lbm_solver* a = slabs[k];
+        if (!a || !a->zghost || a->dom.nx != slabs[0]->dom.nx || a->dom.ny != slabs[0]->dom.ny ||
+            a->storage != slabs[0]->storage) {
+            set_error("lbm_zslab_plan_create: needs z-slab solvers of one x-y size and storage");
+            return LBM_ERR_INVALID;
+        }
+    }
+    const int64_t pl = (int64_t)slabs[0]->dom.nx * slabs[0]->dom.ny;
+    std::vector<SlabJob> jobs[2];
+    for (int k = 0; k < n; ++k) {
+        lbm_solver* lo = slabs[k];
+        lbm_solver* up = slabs[(k + 1) % n];
+        void *lo_top[5], *lo_ghost[5], *up_ghost[5], *up_bot[5];
+        int64_t b = 0;
+        int rc;
+        if ((rc = lbm_zslab_slots(lo, lo->dom.nz - 2, -1, lo_top, &b)) != LBM_OK ||
+            (rc = lbm_zslab_slots(lo, lo->dom.nz - 1, 1, lo_ghost, &b)) != LBM_OK ||
+            (rc = lbm_zslab_slots(up, 0, -1, up_ghost, &b)) != LBM_OK ||
+            (rc = lbm_zslab_slots(up, 1, 1, up_bot, &b)) != LBM_OK)
+            return rc;
+        const int64_t lo_off = (int64_t)(lo->dom.nz - 2) * pl, up_off = pl;
+        int kd = 0, ku = 0;
+        for (int q = 0; q < 19; ++q) {
+            if (lbm::cz(q) == -1) {
+                jobs[0].push_back({up_ghost[kd], lo_top[kd], nullptr, nullptr, pl, 0, 0});
+                jobs[1].push_back({lo_top[kd], up_ghost[kd], lo->use_flags ? lo->flags + lo_off : nullptr,
+                                   lo->links + lo_off, pl, lbm::opp(q), 0});
+                ++kd;
+            } else if (lbm::cz(q) == 1) {
+                jobs[0].push_back({lo_ghost[ku], up_bot[ku], nullptr, nullptr, pl, 0, 0});
+                jobs[1].push_back({up_bot[ku], lo_ghost[ku], up->use_flags ? up->flags + up_off : nullptr,
+                                   up->links + up_off, pl, lbm::opp(q), 0});
+                ++ku;
+            }
+        }
+    }
+    auto* p = new lbm_zslab_plan();
+    p->njobs = (int)jobs[0].size();
+    p->esize = (int)slabs[0]->esize;
+    p->elems = pl;
+    for (int ph = 0; ph < 2; ++ph) {
+        if (cudaMalloc((void**)&p->d_jobs[ph], sizeof(SlabJob) * jobs[ph].size()) != cudaSuccess ||
+            cudaMemcpy(p->d_jobs[ph], jobs[ph].data(), sizeof(SlabJob) * jobs[ph].size(), cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+            lbm_zslab_plan_destroy(p);
+            set_error("lbm_zslab_plan_create: allocation failed");
+            return LBM_ERR_ALLOC;
+        }
+    }
+    *out = p;
+    return LBM_OK;
+}
+
+int lbm_zslab_plan_exchange(lbm_zslab_plan* p, int phase, void* stream) {
+    if (!p || (phase != 0 && phase != 1)) { set_error("lbm_zslab_plan_exchange: bad argument"); return LBM_ERR_INVALID; }
+    const dim3 grid((unsigned)std::min<int64_t>((p->elems + 255) / 256, 1024), (unsigned)p->njobs);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (p->esize == 4) zslab_jobs<uint32_t><<<grid, 256, 0, st>>>(p->d_jobs[phase]);
+    else zslab_jobs<uint16_t><<<grid, 256, 0, st>>>(p->d_jobs[phase]);
+    CK(cudaGetLastError());
+    return LBM_OK;
+}
+
+int lbm_zslab_plan_destroy(lbm_zslab_plan* p) {
+    if (!p) return LBM_OK;
+    cudaFree(p->d_jobs[0]);
+    cudaFree(p->d_jobs[1]);
+    delete p;
+    return LBM_OK;
+}
+
+int lbm_step_parity(lbm_solver* s, int* parity) {
+    if (!s || !parity) { set_error("lbm_step_parity: null argument"); return LBM_ERR_INVALID; }
+    *parity = s->parity;
+    return LBM_OK;
+}
+
 int lbm_solver_stream(lbm_solver* s, void** stream) {
     if (!s || !stream) { set_error("lbm_solver_stream: null argument"); return LBM_ERR_INVALID; }
     *stream = s->stream;
@@ -850,6 +1076,10 @@ int lbm_batch_create(lbm_solver* const* solvers, int32_t n, void* stream, lbm_ba
         if (!s) { set_error("lbm_batch_create: null solver"); return LBM_ERR_INVALID; }
         if (!is_aa(s) || is_ref_push(s) || s->storage != LBM_STORE_F32) {
             set_error("lbm_batch_create: instances must be Legacy/Hybrid, FP32, halfway bounce-back");
+            return LBM_ERR_UNSUPPORTED;
+        }
+        if (s->zghost) {
+            set_error("lbm_batch_create: z-slab solvers (ghost planes) cannot be batched");
             return LBM_ERR_UNSUPPORTED;
         }
         if (s->N % 2 != 0 || (uint64_t)s->N * 19u >= (1ull << 32)) {

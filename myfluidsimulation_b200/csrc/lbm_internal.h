@@ -27,6 +27,10 @@ struct AAParams {
     int macro;
     double* partials;        // [gridDim.x][NSTAT] when stats != 0
     int stats;
+    // cells stepped by aa_even / aa_odd: [first, first + cells), whole planes;
+    // all N, or the interior planes of a z-slab whose first and last planes are
+    // ghost copies of the neighbouring slabs' boundary planes
+    int64_t first, cells;
 };
 
 // Parameters of one HOME step (moment-only, two buffers).

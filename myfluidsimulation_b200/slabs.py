@@ -1,0 +1,306 @@
+"""z-slab decomposition of the Legacy/Hybrid (AA) step.
+
+The domain's z planes are split into slabs.  Each slab solver holds its planes
+plus one ghost plane at each end (`lbm_set_z_ghosts`), and steps only its own
+planes.  The AA even step is local.  Around each odd step the 5 slot planes
+crossing each slab face (directions with c_z = +-1) travel twice:
+  phase 0, before the odd step: boundary plane -> the neighbour's ghost plane;
+  phase 1, after it: ghost plane -> its owner's boundary plane, for the cells
+           whose link across the face streams (a population that a boundary
+           cell bounced back off a solid neighbour stays where it is).
+Nothing else is exchanged, and every cell computes exactly what it would in one
+grid, so a decomposed run equals the single-grid run bit for bit.
+
+`SlabSet` keeps all slabs on one GPU, with device copies as the exchange.
+`DistSlab` keeps one slab per process (torch.distributed, NCCL between GPUs;
+any backend works for the plan), exchanging with point-to-point sends.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import BC_PERIODIC, METHOD_LEGACY, STORE_F32, check, lib
+from .solvers import Solver
+
+__all__ = ["slab_bounds", "exchange_plan", "exchange", "with_ghosts", "SlabSet", "DistSlab"]
+
+
+def slab_bounds(nz: int, parts: int):
+    """[z0, z1) of each slab: nz planes in `parts` nearly equal runs."""
+    if parts < 1 or parts > nz:
+        raise ValueError("need 1 <= parts <= nz")
+    cuts = [nz * k // parts for k in range(parts + 1)]
+    return [(cuts[k], cuts[k + 1]) for k in range(parts)]
+
+
+def with_ghosts(a, z0: int, z1: int, axis: int = 0):
+    """Planes z0-1 .. z1 of a periodic field (the slab and its two ghosts)."""
+    a = np.asarray(a)
+    nz = a.shape[axis]
+    idx = [(z0 - 1) % nz] + list(range(z0, z1)) + [z1 % nz]
+    return np.ascontiguousarray(np.take(a, idx, axis=axis))
+
+
+# planes of a slab solver with L planes: 0 ghost below, 1 first own, L-2 last own, L-1 ghost above
+def exchange_plan(phase: int, rank: int, world: int):
+    """Point-to-point transfers of one rank for one phase:
+    (kind, peer, plane, cz): kind 'send' or 'recv'; plane one of
+    'ghost_lo', 'first', 'last', 'ghost_hi'; cz the direction set (+1/-1).
+    Sends precede receives in the list; a pair of ranks posts matching ops."""
+    lo, hi = (rank - 1) % world, (rank + 1) % world
+    if phase == 0:
+        return [("send", hi, "last", -1), ("send", lo, "first", +1),
+                ("recv", lo, "ghost_lo", -1), ("recv", hi, "ghost_hi", +1)]
+    if phase == 1:
+        return [("send", lo, "ghost_lo", -1), ("send", hi, "ghost_hi", +1),
+                ("recv", hi, "last", -1), ("recv", lo, "first", +1)]
+    raise ValueError("phase is 0 or 1")
+
+
+def exchange(views, phase: int, rank: int, world: int, dist, group=None, recv_views=None):
+    """Run one phase of the plan with torch.distributed point-to-point ops.
+    views[(plane, cz)]: the 5 tensors (slot planes) of that plane and
+    direction set, in direction order, on this rank; recv_views (optional)
+    redirects receives of a (plane, cz) into other tensors (staging)."""
+    ops = []
+    for kind, peer, plane, cz in exchange_plan(phase, rank, world):
+        fn = dist.isend if kind == "send" else dist.irecv
+        peer_g = dist.get_global_rank(group, peer) if group is not None else peer
+        ts = views[(plane, cz)]
+        if kind == "recv" and recv_views and (plane, cz) in recv_views:
+            ts = recv_views[(plane, cz)]
+        for t in ts:
+            ops.append(dist.P2POp(fn, t, peer_g, group))
+    for w in dist.batch_isend_irecv(ops):
+        w.wait()
+
+
+def _slot_ptrs(solver: Solver, plane: int, cz: int):
+    ptrs = (C.c_void_p * 5)()
+    nb = C.c_int64()
+    check(lib().lbm_zslab_slots(solver._h, int(plane), int(cz), ptrs, C.byref(nb)))
+    return [p for p in ptrs], nb.value
+
+
+def _parity(solver: Solver) -> int:
+    v = C.c_int()
+    check(lib().lbm_step_parity(solver._h, C.byref(v)))
+    return v.value
+
+
+class SlabSet:
+    """All slabs of one grid on this GPU (one stream); the single-device image of
+    the multi-GPU layout.  Fields are given and returned for the whole grid."""
+
+    def __init__(self, nx, ny, nz, tau, parts, force=(0.0, 0.0, 0.0), method=METHOD_LEGACY, storage=STORE_F32,
+                 bc=BC_PERIODIC, inlet_u=0.0, stream=None):
+        import torch
+        self.shape = (nz, ny, nx)
+        self.bounds = slab_bounds(nz, parts)
+        self.stream = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self.slabs = []
+        self._plan = None
+        for z0, z1 in self.bounds:
+            s = Solver(nx, ny, z1 - z0 + 2, tau, force, method=method, storage=storage, bc=bc, inlet_u=inlet_u,
+                       stream=self.stream)
+            check(lib().lbm_set_z_ghosts(s._h, 1))
+            self.slabs.append(s)
+
+    def _drop_plan(self):
+        if self._plan:
+            check(lib().lbm_zslab_plan_destroy(self._plan))
+            self._plan = None
+
+    def set_solid_mask(self, mask):
+        m = np.asarray(mask, np.uint8).reshape(self.shape)
+        for s, (z0, z1) in zip(self.slabs, self.bounds):
+            s.set_solid_mask(with_ghosts(m, z0, z1))
+        self._drop_plan()
+
+    def set_legacy_mapping(self, band):
+        b = np.asarray(band, np.uint8).reshape(self.shape)
+        for s, (z0, z1) in zip(self.slabs, self.bounds):
+            s.set_legacy_mapping(with_ghosts(b, z0, z1))
+        self._drop_plan()
+
+    def reinit_from_host(self, rho=None, ux=None, uy=None, uz=None):
+        for s, (z0, z1) in zip(self.slabs, self.bounds):
+            s.reinit_from_host(*[None if a is None else with_ghosts(np.asarray(a, np.float32).reshape(self.shape),
+                                                                     z0, z1) for a in (rho, ux, uy, uz)])
+
+    def enable_stats(self, on=True):
+        for s in self.slabs:
+            s.enable_stats(on)
+
+    def set_shear_omega(self, omega_s):
+        for s in self.slabs:
+            s.set_shear_omega(omega_s)
+
+    def set_macro_output(self, on=True):
+        for s in self.slabs:
+            s.set_macro_output(on)
+
+    def _ensure_plan(self):
+        # every face in one launch per phase (lbm_zslab_plan_*), built after the mask and band
+        if self._plan is None:
+            hs = (C.c_void_p * len(self.slabs))(*[s._h.value for s in self.slabs])
+            p = C.c_void_p()
+            check(lib().lbm_zslab_plan_create(hs, len(self.slabs), C.byref(p)))
+            self._plan = p
+
+    def _exchange(self, phase):
+        self._ensure_plan()
+        check(lib().lbm_zslab_plan_exchange(self._plan, phase, C.c_void_p(self.stream)))
+
+    def exchange_pairwise(self, phase):
+        """The same transfers as one lbm_zslab_exchange per face."""
+        n = len(self.slabs)
+        for k in range(n):
+            check(lib().lbm_zslab_exchange(self.slabs[k]._h, self.slabs[(k + 1) % n]._h, phase,
+                                           C.c_void_p(self.stream)))
+
+    def graph(self, n: int = 2):
+        """A torch CUDA graph of n steps (n even: the step parity comes back).
+        Needs a stream other than the legacy default one; replay() advances the
+        device state by n steps (the solvers' host-side step counters do not move)."""
+        import torch
+        if n % 2 or n < 2:
+            raise ValueError("n must be even")
+        self._ensure_plan()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=torch.cuda.ExternalStream(self.stream)):
+            self.step(n)
+        return g
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            odd = _parity(self.slabs[0]) == 1
+            if odd:
+                self._exchange(0)
+            for s in self.slabs:
+                s.step(1)
+            if odd:
+                self._exchange(1)
+
+    def synchronize(self):
+        for s in self.slabs:
+            s.synchronize()
+
+    def macros(self):
+        parts = [s.macros() for s in self.slabs]
+        return tuple(np.concatenate([p[k][1:-1] for p in parts], axis=0) for k in range(4))
+
+    def state(self):
+        """Populations of the whole grid in the natural layout (after an even step count)."""
+        return np.concatenate([s.state()[:, 1:-1] for s in self.slabs], axis=1)
+
+    def stats(self) -> dict:
+        out = {}
+        for s in self.slabs:
+            for k, v in s.stats().items():
+                out[k] = out.get(k, 0.0) + v
+        out["ke_mean"] = out["ke_sum"] / int(np.prod(self.shape))
+        return out
+
+    def close(self):
+        self._drop_plan()
+        for s in self.slabs:
+            s.close()
+        self.slabs = []
+
+
+def _device_view(ptr: int, nbytes: int, device):
+    """A uint8 torch tensor over raw device memory (no copy)."""
+    import torch
+
+    class _Mem:
+        __cuda_array_interface__ = {"shape": (nbytes,), "typestr": "|u1", "data": (ptr, False), "version": 3,
+                                    "strides": None}
+
+    return torch.as_tensor(_Mem(), device=device)
+
+
+class DistSlab:
+    """This process's slab of a grid split across the ranks of a torch.distributed
+    group (one GPU per rank).  The solver runs on torch's current stream, so the
+    point-to-point transfers (queued by torch on its communication stream after
+    the work already on the current stream) order correctly with the steps."""
+
+    def __init__(self, nx, ny, nz, tau, force=(0.0, 0.0, 0.0), method=METHOD_LEGACY, storage=STORE_F32,
+                 bc=BC_PERIODIC, inlet_u=0.0, group=None, dist=None):
+        import torch
+        if dist is None:
+            import torch.distributed as dist
+        self.dist, self.group = dist, group
+        self.rank, self.world = dist.get_rank(group), dist.get_world_size(group)
+        self.shape = (nz, ny, nx)
+        self.z0, self.z1 = slab_bounds(nz, self.world)[self.rank]
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        self.solver = Solver(nx, ny, self.z1 - self.z0 + 2, tau, force, method=method, storage=storage, bc=bc,
+                             inlet_u=inlet_u, stream=torch.cuda.current_stream().cuda_stream)
+        check(lib().lbm_set_z_ghosts(self.solver._h, 1))
+        L = self.z1 - self.z0 + 2
+        planes = {"ghost_lo": 0, "first": 1, "last": L - 2, "ghost_hi": L - 1}
+        self.planes = planes
+        self.views = {}
+        for name, pl in planes.items():
+            for cz in (+1, -1):
+                ptrs, nb = _slot_ptrs(self.solver, pl, cz)
+                self.views[(name, cz)] = [_device_view(p, nb, self.device) for p in ptrs]
+        # phase 1 lands in staging first: only the values the neighbour's cells
+        # wrote are taken (lbm_zslab_merge), a bounced-back population stays
+        self.staging = {key: [torch.empty_like(t) for t in self.views[key]] for key in (("last", -1), ("first", 1))}
+
+    def _exchange(self, phase):
+        if self.world == 1:
+            check(lib().lbm_zslab_exchange(self.solver._h, self.solver._h, phase, C.c_void_p(self.solver.stream)))
+            return
+        if phase == 0:
+            exchange(self.views, 0, self.rank, self.world, self.dist, self.group)
+            return
+        exchange(self.views, 1, self.rank, self.world, self.dist, self.group, recv_views=self.staging)
+        for (name, cz), ts in self.staging.items():
+            src = (C.c_void_p * 5)(*[t.data_ptr() for t in ts])
+            check(lib().lbm_zslab_merge(self.solver._h, self.planes[name], cz, src,
+                                        C.c_void_p(self.solver.stream)))
+
+    def set_solid_mask(self, mask):
+        self.solver.set_solid_mask(with_ghosts(np.asarray(mask, np.uint8).reshape(self.shape), self.z0, self.z1))
+
+    def set_legacy_mapping(self, band):
+        self.solver.set_legacy_mapping(with_ghosts(np.asarray(band, np.uint8).reshape(self.shape), self.z0, self.z1))
+
+    def reinit_from_host(self, rho=None, ux=None, uy=None, uz=None):
+        self.solver.reinit_from_host(*[None if a is None else with_ghosts(
+            np.asarray(a, np.float32).reshape(self.shape), self.z0, self.z1) for a in (rho, ux, uy, uz)])
+
+    def step(self, n: int = 1):
+        for _ in range(n):
+            odd = _parity(self.solver) == 1
+            if odd:
+                self._exchange(0)
+            self.solver.step(1)
+            if odd:
+                self._exchange(1)
+
+    def set_shear_omega(self, omega_s):
+        self.solver.set_shear_omega(omega_s)
+
+    def enable_stats(self, on=True):
+        self.solver.enable_stats(on)
+
+    def synchronize(self):
+        self.solver.synchronize()
+
+    def macros(self):
+        """This rank's planes z0..z1-1 of rho, ux, uy, uz."""
+        return tuple(m[1:-1] for m in self.solver.macros())
+
+    def state(self):
+        """This rank's populations (natural layout after an even step count)."""
+        return self.solver.state()[:, 1:-1]
+
+    def close(self):
+        self.solver.close()

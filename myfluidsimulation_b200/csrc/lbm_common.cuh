@@ -113,20 +113,25 @@ struct StoreF32 {
     using T = float;
     static constexpr int kId = 0;
     __device__ __forceinline__ static float ld(const T* p, int q, float r0) { return __ldg(p); }
-    __device__ __forceinline__ static void st(T* p, int q, float r0, float v) { *p = v; }
+    // Every population store is streaming (.cs, evict first): nothing reads a
+    // stored slot again in the same launch, and the step's state is larger than
+    // L2, so the lines L2 keeps are those still to be gathered (the odd step's
+    // x-shifted rows are read by two warps).  Measured on B200: the duct's odd
+    // step 138.8 -> 134.7 us, the 512^3 F16 even step 1.81 -> 1.71 ms.
+    __device__ __forceinline__ static void st(T* p, int q, float r0, float v) { __stcs(p, v); }
     __device__ __forceinline__ static void ld4(const T* p, int q, float r0, float* o) {
         const float4 v = *reinterpret_cast<const float4*>(p);
         o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
     }
     __device__ __forceinline__ static void st4(T* p, int q, float r0, const float* v) {
-        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+        __stcs(reinterpret_cast<float4*>(p), make_float4(v[0], v[1], v[2], v[3]));
     }
     __device__ __forceinline__ static void ld2(const T* p, int q, float r0, float* o) {
         const float2 v = *reinterpret_cast<const float2*>(p);
         o[0] = v.x; o[1] = v.y;
     }
     __device__ __forceinline__ static void st2(T* p, int q, float r0, const float* v) {
-        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+        __stcs(reinterpret_cast<float2*>(p), make_float2(v[0], v[1]));
     }
 };
 
@@ -142,7 +147,7 @@ struct StoreF16 {
         return __half2float(*p) * kF16Inv + wq(q) * r0;
     }
     __device__ __forceinline__ static void st(T* p, int q, float r0, float v) {
-        *p = __float2half_rn((v - wq(q) * r0) * kF16Scale);
+        __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn((v - wq(q) * r0) * kF16Scale)));
     }
     __device__ __forceinline__ static void ld4(const T* p, int q, float r0, float* o) {
         const uint2 raw = *reinterpret_cast<const uint2*>(p);
@@ -159,7 +164,7 @@ struct StoreF16 {
         uint2 raw;
         raw.x = *reinterpret_cast<uint32_t*>(&a);
         raw.y = *reinterpret_cast<uint32_t*>(&b);
-        *reinterpret_cast<uint2*>(p) = raw;
+        __stcs(reinterpret_cast<uint2*>(p), raw);
     }
     __device__ __forceinline__ static void ld2(const T* p, int q, float r0, float* o) {
         const float2 f = __half22float2(*reinterpret_cast<const __half2*>(p));
@@ -179,7 +184,7 @@ struct StoreBF16 {
         return __bfloat162float(*p) + wq(q) * r0;
     }
     __device__ __forceinline__ static void st(T* p, int q, float r0, float v) {
-        *p = __float2bfloat16_rn(v - wq(q) * r0);
+        __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(__float2bfloat16_rn(v - wq(q) * r0)));
     }
     __device__ __forceinline__ static void ld4(const T* p, int q, float r0, float* o) {
         const uint2 raw = *reinterpret_cast<const uint2*>(p);
@@ -196,7 +201,7 @@ struct StoreBF16 {
         uint2 raw;
         raw.x = *reinterpret_cast<uint32_t*>(&a);
         raw.y = *reinterpret_cast<uint32_t*>(&b);
-        *reinterpret_cast<uint2*>(p) = raw;
+        __stcs(reinterpret_cast<uint2*>(p), raw);
     }
     __device__ __forceinline__ static void ld2(const T* p, int q, float r0, float* o) {
         const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));

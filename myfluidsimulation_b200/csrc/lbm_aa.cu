@@ -82,6 +82,58 @@ __device__ __forceinline__ void collide(float (&f)[19], const Cell& c, float ome
     pair(17, 16, c.uy - c.uz, r2);
 }
 
+// The same two functions in the stored units of the narrow forms,
+// g_q = (f_q - w_q rho0) S: sum g = S (rho - rho0) and sum c g = S rho u (the
+// weights' first moment vanishes), and the equilibrium in those units is
+//   geq_(+-) = S [w (rho - rho0) + w rho (4.5 t^2 - 1.5 u^2)] +- 3 S w rho t.
+// The populations are never converted back to f, so a step costs no
+// conversion arithmetic per population and rho - rho0 keeps its low bits.
+__device__ __forceinline__ Cell moments_g(const float (&g)[19], float fx, float fy, float fz, float r0, float invS,
+                                          float& dr) {
+    const float s12 = g[1] + g[2], d12 = g[1] - g[2];
+    const float s34 = g[3] + g[4], d34 = g[3] - g[4];
+    const float s56 = g[5] + g[6], d56 = g[5] - g[6];
+    const float s7 = g[7] + g[10], d7 = g[7] - g[10];
+    const float s9 = g[9] + g[8], d9 = g[9] - g[8];
+    const float s11 = g[11] + g[14], d11 = g[11] - g[14];
+    const float s13 = g[13] + g[12], d13 = g[13] - g[12];
+    const float s15 = g[15] + g[18], d15 = g[15] - g[18];
+    const float s17 = g[17] + g[16], d17 = g[17] - g[16];
+    Cell c;
+    dr = (g[0] + ((s12 + s34) + (s56 + s7)) + ((s9 + s11) + (s13 + s15) + s17)) * invS;
+    c.r = r0 + dr;
+    const float jx = ((d12 + d7) + (d9 + d11) + d13) * invS;
+    const float jy = ((d34 + d7) - d9 + (d15 + d17)) * invS;
+    const float jz = ((d56 + d11) - d13 + (d15 - d17)) * invS;
+    const float inv = c.r > 0.f ? 1.0f / c.r : 0.f;
+    c.ux = jx * inv + fx;
+    c.uy = jy * inv + fy;
+    c.uz = jz * inv + fz;
+    return c;
+}
+
+__device__ __forceinline__ void collide_g(float (&g)[19], const Cell& c, float dr, float omega, float S) {
+    const float A1 = -1.5f * (c.ux * c.ux + c.uy * c.uy + c.uz * c.uz);
+    const float r0 = mulk(c.r, K3_HI, K3_LO), r1 = mulk(c.r, K18_HI, K18_LO), r2 = mulk(c.r, K36_HI, K36_LO);
+    const float d0 = mulk(dr, K3_HI, K3_LO), d1 = mulk(dr, K18_HI, K18_LO), d2 = mulk(dr, K36_HI, K36_LO);
+    auto pair = [&](int qp, int qm, float t, float wr, float wd) {
+        const float sym = S * fmaf(wr, fmaf(4.5f * t, t, A1), wd);
+        const float asym = S * (3.0f * wr * t);
+        g[qp] = fmaf(omega, (sym + asym) - g[qp], g[qp]);
+        g[qm] = fmaf(omega, (sym - asym) - g[qm], g[qm]);
+    };
+    g[0] = fmaf(omega, S * fmaf(r0, A1, d0) - g[0], g[0]);
+    pair(1, 2, c.ux, r1, d1);
+    pair(3, 4, c.uy, r1, d1);
+    pair(5, 6, c.uz, r1, d1);
+    pair(7, 10, c.ux + c.uy, r2, d2);
+    pair(9, 8, c.ux - c.uy, r2, d2);
+    pair(11, 14, c.ux + c.uz, r2, d2);
+    pair(13, 12, c.ux - c.uz, r2, d2);
+    pair(15, 18, c.uy + c.uz, r2, d2);
+    pair(17, 16, c.uy - c.uz, r2, d2);
+}
+
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 // Momentum exchanged with obstacle cells along the solid links of one cell.
@@ -101,6 +153,14 @@ __device__ __noinline__ void add_drag(double* acc, const float* o, uint32_t lk, 
     }
 }
 
+// add_drag for populations in stored units (narrow forms): f = g / S + w rho0.
+__device__ __noinline__ void add_drag_g(double* acc, const float* o, float invS, float r0, uint32_t lk,
+                                        const uint8_t* flags, int x, int y, int z, int nx, int ny, int nz, int duct) {
+    float f[19];
+    for (int q = 0; q < 19; ++q) f[q] = o[q] * invS + wq(q) * r0;
+    add_drag(acc, f, lk, flags, x, y, z, nx, ny, nz, duct);
+}
+
 __device__ __forceinline__ void add_cell_stats(double (&acc)[NSTAT], const Cell& c) {
     acc[0] += (double)c.r;
     acc[1] += 0.5 * ((double)c.ux * c.ux + (double)c.uy * c.uy + (double)c.uz * c.uz);
@@ -113,6 +173,10 @@ __device__ __forceinline__ void add_cell_stats(double (&acc)[NSTAT], const Cell&
 // (rho, (u_in,0,0)) of a direction with c_x = +1 is w rho (1 + 3u + 3u^2);
 // `kin` = 1 + 3u + 3u^2.
 __device__ __forceinline__ float inlet_value(int q, float r, float kin) { return wq(q) * r * kin; }
+// the same in stored units: S w (rho kin - rho0)
+__device__ __forceinline__ float inlet_g(int q, float r, float kin, float r0, float S) {
+    return S * (wq(q) * fmaf(r, kin, -r0));
+}
 
 // ---------------------------------------------------------------------------
 // Even step: local.  VEC consecutive cells per thread.
@@ -127,10 +191,14 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
     const IDX N = (IDX)p.N;
     const float kin = 1.0f + 3.0f * p.u_in + 3.0f * p.u_in * p.u_in;
     {
+        constexpr bool SH = ST::kId != 0;   // narrow forms: compute in stored units
         const IDX id = v * VEC;
         float a[19][VEC];
 #pragma unroll
-        for (int q = 0; q < 19; ++q) ldv<ST, VEC>(f + (IDX)q * N + id, q, p.rho0, a[q]);
+        for (int q = 0; q < 19; ++q) {
+            if constexpr (SH) ldv_raw<ST, VEC>(f + (IDX)q * N + id, a[q]);
+            else ldv<ST, VEC>(f + (IDX)q * N + id, q, p.rho0, a[q]);
+        }
         uint32_t fl4 = 0;
         if constexpr (MASK) {
             if constexpr (VEC == 4) fl4 = *reinterpret_cast<const uint32_t*>(p.flags + id);
@@ -146,21 +214,27 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
             float c[19];
 #pragma unroll
             for (int q = 0; q < 19; ++q) c[q] = a[q][l];
-            const Cell m = moments(c, p.fx, p.fy, p.fz);
+            float dr = 0.f;
+            const Cell m = SH ? moments_g(c, p.fx, p.fy, p.fz, p.rho0, Raw<ST>::invS, dr) : moments(c, p.fx, p.fy, p.fz);
             const bool solid = MASK && (fl & F_SOLID);
             const float om = (p.hybrid && !(fl & F_BAND)) ? p.omega_s : p.omega;
             float o[19];
 #pragma unroll
             for (int q = 0; q < 19; ++q) o[q] = c[q];
-            collide(o, m, om);
+            if constexpr (SH) collide_g(o, m, dr, om, Raw<ST>::S);
+            else collide(o, m, om);
             if (STATS && !solid) {
                 add_cell_stats(acc, m);
                 if (MASK && (fl & F_TOUCH)) {
                     const IDX xg = id + l;
                     const int xi = (int)(xg % (IDX)p.nx);
                     const IDX row = xg / (IDX)p.nx;
-                    add_drag(acc, o, p.links[xg], p.flags, xi, (int)(row % (IDX)p.ny), (int)(row / (IDX)p.ny),
-                             p.nx, p.ny, p.nz, p.duct);
+                    if constexpr (SH)
+                        add_drag_g(acc, o, Raw<ST>::invS, p.rho0, p.links[xg], p.flags, xi, (int)(row % (IDX)p.ny),
+                                   (int)(row / (IDX)p.ny), p.nx, p.ny, p.nz, p.duct);
+                    else
+                        add_drag(acc, o, p.links[xg], p.flags, xi, (int)(row % (IDX)p.ny), (int)(row / (IDX)p.ny),
+                                 p.nx, p.ny, p.nz, p.duct);
                 }
             }
             const int x = x0 + l;
@@ -168,7 +242,7 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
                 float v = o[q];
-                if (cx(q) < 0) v = at_in ? inlet_value(q, m.r, kin) : v;
+                if (cx(q) < 0) v = at_in ? (SH ? inlet_g(q, m.r, kin, p.rho0, Raw<ST>::S) : inlet_value(q, m.r, kin)) : v;
                 if (cx(q) > 0) v = at_out ? o[opp(q)] : v;
                 // a solid cell keeps its populations (legacy.cu:72-76): slot opp(q) gets its own value
                 a[q][l] = solid ? c[opp(q)] : v;
@@ -179,7 +253,10 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
             mw[l] = solid ? 0.f : m.uz;
         }
 #pragma unroll
-        for (int q = 0; q < 19; ++q) stv<ST, VEC>(f + (IDX)opp(q) * N + id, q, p.rho0, a[q]);
+        for (int q = 0; q < 19; ++q) {
+            if constexpr (SH) stv_raw<ST, VEC>(f + (IDX)opp(q) * N + id, a[q]);
+            else stv<ST, VEC>(f + (IDX)opp(q) * N + id, q, p.rho0, a[q]);
+        }
         if constexpr (MACRO) {
             stv<StoreF32, VEC>(p.rho + id, 0, 0.f, mr);
             stv<StoreF32, VEC>(p.ux + id, 0, 0.f, mu);
@@ -231,6 +308,7 @@ struct Nbr {
 template <class ST, bool MASK, int MODE, class IDX>
 __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, double (&acc)[NSTAT]) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
+    constexpr bool SH = ST::kId != 0;   // narrow forms: compute in stored units
     using T = typename ST::T;
     T* __restrict__ f = static_cast<T*>(p.f);
     const IDX N = (IDX)p.N;
@@ -256,28 +334,36 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, doub
             // stream, the value was left in the cell's own slot q
             const bool nn = (lk >> opp(q)) & 1u;
             const IDX src = nn ? ((IDX)q * N + id) : ((IDX)opp(q) * N + nb.at(-cx(q), -cy(q), -cz(q)));
-            c[q] = ST::ld(f + src, q, p.rho0);
+            if constexpr (SH) c[q] = Raw<ST>::ld(f + src);
+            else c[q] = ST::ld(f + src, q, p.rho0);
         }
-        const Cell m = moments(c, p.fx, p.fy, p.fz);
+        float dr = 0.f;
+        const Cell m = SH ? moments_g(c, p.fx, p.fy, p.fz, p.rho0, Raw<ST>::invS, dr) : moments(c, p.fx, p.fy, p.fz);
         const float om = (p.hybrid && !(fl & F_BAND)) ? p.omega_s : p.omega;
         float o[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) o[q] = c[q];
-        collide(o, m, om);
+        if constexpr (SH) collide_g(o, m, dr, om, Raw<ST>::S);
+        else collide(o, m, om);
         const bool at_in = p.duct && x == 0, at_out = p.duct && x == nx - 1;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             const bool nn = (lk >> q) & 1u;
             float v = o[q];
-            if (cx(q) < 0) v = (nn && at_in) ? inlet_value(q, m.r, kin) : v;
+            if (cx(q) < 0)
+                v = (nn && at_in) ? (SH ? inlet_g(q, m.r, kin, p.rho0, Raw<ST>::S) : inlet_value(q, m.r, kin)) : v;
             if (cx(q) > 0) v = (nn && at_out) ? o[opp(q)] : v;
             const IDX dst = nn ? ((IDX)opp(q) * N + id) : ((IDX)q * N + nb.at(cx(q), cy(q), cz(q)));
-            ST::st(f + dst, q, p.rho0, v);
+            if constexpr (SH) Raw<ST>::st(f + dst, v);
+            else ST::st(f + dst, q, p.rho0, v);
         }
         if (MACRO) { p.rho[id] = m.r; p.ux[id] = m.ux; p.uy[id] = m.uy; p.uz[id] = m.uz; }
         if (STATS) {
             add_cell_stats(acc, m);
-            if (MASK && (fl & F_TOUCH)) add_drag(acc, o, lk, p.flags, x, y, z, nx, ny, nz, p.duct);
+            if (MASK && (fl & F_TOUCH)) {
+                if constexpr (SH) add_drag_g(acc, o, Raw<ST>::invS, p.rho0, lk, p.flags, x, y, z, nx, ny, nz, p.duct);
+                else add_drag(acc, o, lk, p.flags, x, y, z, nx, ny, nz, p.duct);
+            }
         }
     }
 }

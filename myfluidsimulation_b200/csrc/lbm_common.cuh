@@ -215,6 +215,85 @@ struct StoreBF16 {
 };
 
 // vector load/store of VEC consecutive cells of one population plane
+// The narrow forms in their stored units, g = (f - w_q rho0) * S (S = 2^10 for
+// F16, 1 for BF16), for steps that compute in those units: no conversion back
+// to f on load and none on store, and no cancellation against w_q rho0.
+template <class ST> struct Raw;
+template <> struct Raw<StoreF32> {   // FP32 stores f itself (S = 1, no shift)
+    using T = float;
+    static constexpr float S = 1.0f, invS = 1.0f;
+    __device__ __forceinline__ static float ld(const T* p) { return __ldg(p); }
+    __device__ __forceinline__ static void st(T* p, float g) { __stcs(p, g); }
+};
+template <> struct Raw<StoreF16> {
+    using T = __half;
+    static constexpr float S = kF16Scale, invS = kF16Inv;
+    __device__ __forceinline__ static float ld(const T* p) { return __half2float(*p); }
+    __device__ __forceinline__ static void st(T* p, float g) {
+        __stcs(reinterpret_cast<unsigned short*>(p), __half_as_ushort(__float2half_rn(g)));
+    }
+    __device__ __forceinline__ static void ld4(const T* p, float* o) {
+        const uint2 raw = *reinterpret_cast<const uint2*>(p);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+    __device__ __forceinline__ static void st4(T* p, const float* v) {
+        __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+        uint2 raw;
+        raw.x = *reinterpret_cast<uint32_t*>(&a);
+        raw.y = *reinterpret_cast<uint32_t*>(&b);
+        __stcs(reinterpret_cast<uint2*>(p), raw);
+    }
+    __device__ __forceinline__ static void ld2(const T* p, float* o) {
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(p));
+        o[0] = a.x; o[1] = a.y;
+    }
+    __device__ __forceinline__ static void st2(T* p, const float* v) {
+        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(v[0], v[1]);
+    }
+};
+template <> struct Raw<StoreBF16> {
+    using T = __nv_bfloat16;
+    static constexpr float S = 1.0f, invS = 1.0f;
+    __device__ __forceinline__ static float ld(const T* p) { return __bfloat162float(*p); }
+    __device__ __forceinline__ static void st(T* p, float g) {
+        __stcs(reinterpret_cast<unsigned short*>(p), __bfloat16_as_ushort(__float2bfloat16_rn(g)));
+    }
+    __device__ __forceinline__ static void ld4(const T* p, float* o) {
+        const uint2 raw = *reinterpret_cast<const uint2*>(p);
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+        const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+        o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+    }
+    __device__ __forceinline__ static void st4(T* p, const float* v) {
+        __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]);
+        uint2 raw;
+        raw.x = *reinterpret_cast<uint32_t*>(&a);
+        raw.y = *reinterpret_cast<uint32_t*>(&b);
+        __stcs(reinterpret_cast<uint2*>(p), raw);
+    }
+    __device__ __forceinline__ static void ld2(const T* p, float* o) {
+        const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(p));
+        o[0] = a.x; o[1] = a.y;
+    }
+    __device__ __forceinline__ static void st2(T* p, const float* v) {
+        *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(v[0], v[1]);
+    }
+};
+template <class ST, int VEC>
+__device__ __forceinline__ void ldv_raw(const typename ST::T* p, float* o) {
+    if constexpr (VEC == 4) Raw<ST>::ld4(p, o);
+    else if constexpr (VEC == 2) Raw<ST>::ld2(p, o);
+    else o[0] = Raw<ST>::ld(p);
+}
+template <class ST, int VEC>
+__device__ __forceinline__ void stv_raw(typename ST::T* p, const float* v) {
+    if constexpr (VEC == 4) Raw<ST>::st4(p, v);
+    else if constexpr (VEC == 2) Raw<ST>::st2(p, v);
+    else Raw<ST>::st(p, v[0]);
+}
+
 template <class ST, int VEC>
 __device__ __forceinline__ void ldv(const typename ST::T* p, int q, float r0, float* o) {
     if constexpr (VEC == 4) ST::ld4(p, q, r0, o);

@@ -379,21 +379,31 @@ int lbm_solver_stream(lbm_solver* s, void** stream);
 /* Parity of the next AA step (0: the local step, 1: the neighbour step). */
 int lbm_step_parity(lbm_solver* s, int* parity);
 
-/* ---- z-slab decomposition (Legacy/Hybrid, halfway bounce-back) ----------- */
+/* ---- z-slab decomposition ------------------------------------------------ */
 
 /* A slab solver of nz planes steps only planes 1..nz-2; planes 0 and nz-1 are
  * ghost copies of the neighbouring slabs' boundary planes (give them the
- * neighbours' mask, band and initial fields).  No reference counterpart: the
- * reference runs one grid on one GPU. */
+ * neighbours' mask, band and initial fields).  Legacy/Hybrid with halfway
+ * bounce-back, and HOME.  No reference counterpart: the reference runs one
+ * grid on one GPU. */
 int lbm_set_z_ghosts(lbm_solver* s, int on);
+/* HOME: device addresses of the 10 moment planes of `plane` in the current
+ * buffer (they move to the other buffer with every step), each *bytes long. */
+int lbm_zslab_moment_planes(lbm_solver* s, int plane, void** ptrs, int64_t* bytes);
+/* Index of this solver's cell 0 in the whole grid (a slab: its plane 0).  Only
+ * HOME's F16/BF16 stochastic rounding reads it, so that a slab draws the same
+ * random bits for a cell as the whole grid does. */
+int lbm_set_index_base(lbm_solver* s, int64_t base);
 /* Device addresses of the 5 slot planes of `plane` whose direction has
  * c_z = cz (+1 or -1), in direction order, each *bytes long: what crosses a
  * slab face in an odd step. */
 int lbm_zslab_slots(lbm_solver* s, int plane, int cz, void** ptrs, int64_t* bytes);
 /* Exchange between two slabs on this device, `lower` below `upper` (periodic
- * wrap: the top slab is `lower` of the bottom one).  Before each odd step
- * (parity 1) call phase 0 on every face: boundary slots -> neighbour's ghost;
- * after it phase 1: ghost slots -> their owner's boundary plane. */
+ * wrap: the top slab is `lower` of the bottom one).  Legacy/Hybrid: before
+ * each odd step (parity 1) call phase 0 on every face: boundary slots ->
+ * neighbour's ghost; after it phase 1: ghost slots -> their owner's boundary
+ * plane.  HOME: phase 0 before every step copies the 10 moment planes of each
+ * boundary plane to the neighbour's ghost; phase 1 does nothing. */
 int lbm_zslab_exchange(lbm_solver* lower, lbm_solver* upper, int phase, void* stream);
 /* Phase 1 for slabs on different devices: after receiving a neighbour's ghost
  * slot planes (5 device buffers, direction order) for `plane` / `cz`, take the

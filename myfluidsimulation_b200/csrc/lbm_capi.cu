@@ -65,6 +65,7 @@ struct lbm_solver {
     lbm::LaunchCfg cfg_even{0, 256}, cfg_odd{0, 256};
     int home_zchunk = 16;
     bool zghost = false;        // z-slab: planes 0 and nz-1 are ghosts, steps cover 1..nz-2
+    uint32_t salt_base = 0;     // HOME narrow stores: index of plane 0 in the whole grid
     // graph cache
     cudaGraphExec_t gexec = nullptr;
     int g_sub = 0, g_parity = -1, g_stats = -1;
@@ -100,6 +101,9 @@ void drop_graph(lbm_solver* s) {
     if (s->gexec) { cudaGraphExecDestroy(s->gexec); s->gexec = nullptr; }
     s->g_sub = 0; s->g_parity = -1; s->g_stats = -1;
 }
+
+// planes a HOME step covers (a z-slab skips its two ghost planes)
+int home_planes(const lbm_solver* s) { return s->zghost ? s->dom.nz - 2 : s->dom.nz; }
 
 float* home_macro_base(lbm_solver* s) {
     // F32 HOME exposes its state directly (d_rho() = m + 0*N, home.cu:355-362)
@@ -157,6 +161,9 @@ lbm::HomeParams home_params(lbm_solver* s, bool stats) {
     p.stats = stats;
     p.zchunk = s->home_zchunk;
     p.ref_bounce = s->bounce == LBM_BOUNCE_REFERENCE;
+    p.zb = s->zghost ? 1 : 0;
+    p.ze = s->zghost ? s->dom.nz - 1 : s->dom.nz;
+    p.salt_base = s->salt_base;
     return p;
 }
 
@@ -198,7 +205,7 @@ static int enqueue_steps(lbm_solver* s, int n) {
             lbm::HomeParams p = home_params(s, st);
             CK(lbm::launch_home_step(p, s->storage, 8, 3, s->stream));
             s->cur ^= 1;
-            if (st) s->last_stat_blocks = lbm::home_num_blocks(s->dom.nx, s->dom.ny, s->dom.nz, s->home_zchunk);
+            if (st) s->last_stat_blocks = lbm::home_num_blocks(s->dom.nx, s->dom.ny, home_planes(s), s->home_zchunk);
         }
         if (st) CK(lbm::launch_finalize_stats(s->partials, s->last_stat_blocks, s->stats, s->stream));
     }
@@ -654,7 +661,7 @@ int lbm_set_home_zchunk(lbm_solver* s, int zchunk) {
     if (s->method != LBM_METHOD_HOME) { set_error("lbm_set_home_zchunk: HOME only"); return LBM_ERR_INVALID; }
     if (zchunk < 1) { set_error("lbm_set_home_zchunk: zchunk must be >= 1"); return LBM_ERR_INVALID; }
     const int z = std::min(zchunk, s->dom.nz);
-    const int need = lbm::home_num_blocks(s->dom.nx, s->dom.ny, s->dom.nz, z);
+    const int need = lbm::home_num_blocks(s->dom.nx, s->dom.ny, home_planes(s), z);
     if (need > s->max_blocks) {
         // per-block statistics partials: grow once the step queue has drained
         CK(cudaStreamSynchronize(s->stream));
@@ -685,8 +692,8 @@ int lbm_set_home_zchunk(lbm_solver* s, int zchunk) {
 
 int lbm_set_z_ghosts(lbm_solver* s, int on) {
     if (!s) { set_error("lbm_set_z_ghosts: null solver"); return LBM_ERR_INVALID; }
-    if (!is_aa(s) || is_ref_push(s)) {
-        set_error("lbm_set_z_ghosts: Legacy/Hybrid with halfway bounce-back only");
+    if (is_ref_push(s)) {
+        set_error("lbm_set_z_ghosts: not for Legacy/Hybrid with the reference's bounce table (two-buffer push)");
         return LBM_ERR_UNSUPPORTED;
     }
     if (on && s->dom.nz < 3) { set_error("lbm_set_z_ghosts: needs nz >= 3 (two ghost planes)"); return LBM_ERR_INVALID; }
@@ -710,12 +717,52 @@ int lbm_zslab_slots(lbm_solver* s, int plane, int cz, void** ptrs, int64_t* byte
     return LBM_OK;
 }
 
+int lbm_zslab_moment_planes(lbm_solver* s, int plane, void** ptrs, int64_t* bytes) {
+    if (!s || !ptrs || !bytes || plane < 0 || plane >= s->dom.nz) {
+        set_error("lbm_zslab_moment_planes: bad argument");
+        return LBM_ERR_INVALID;
+    }
+    if (is_aa(s)) { set_error("lbm_zslab_moment_planes: HOME solvers only"); return LBM_ERR_UNSUPPORTED; }
+    const int64_t pl = (int64_t)s->dom.nx * s->dom.ny;
+    char* base = static_cast<char*>(s->m[s->cur]);
+    for (int c = 0; c < 10; ++c) ptrs[c] = base + s->esize * ((int64_t)c * s->N + (int64_t)plane * pl);
+    *bytes = (int64_t)s->esize * pl;
+    return LBM_OK;
+}
+
+int lbm_set_index_base(lbm_solver* s, int64_t base) {
+    if (!s) { set_error("lbm_set_index_base: null solver"); return LBM_ERR_INVALID; }
+    s->salt_base = (uint32_t)(uint64_t)base;
+    drop_graph(s);
+    return LBM_OK;
+}
+
 int lbm_zslab_exchange(lbm_solver* lower, lbm_solver* upper, int phase, void* stream) {
     if (!lower || !upper || (phase != 0 && phase != 1)) { set_error("lbm_zslab_exchange: bad argument"); return LBM_ERR_INVALID; }
     if (!lower->zghost || !upper->zghost || lower->dom.nx != upper->dom.nx || lower->dom.ny != upper->dom.ny ||
-        lower->storage != upper->storage) {
-        set_error("lbm_zslab_exchange: needs two z-slab solvers of the same x-y size and storage");
+        lower->storage != upper->storage || is_aa(lower) != is_aa(upper)) {
+        set_error("lbm_zslab_exchange: needs two z-slab solvers of the same method family, x-y size and storage");
         return LBM_ERR_INVALID;
+    }
+    if (!is_aa(lower)) {
+        // HOME pulls whole planes of moments: before each step the boundary
+        // planes of the current buffer go to the neighbours' ghosts; nothing
+        // comes back after it
+        if (phase == 1) return LBM_OK;
+        void *lo_top[10], *lo_ghost[10], *up_ghost[10], *up_bot[10];
+        int64_t b = 0;
+        int rc;
+        if ((rc = lbm_zslab_moment_planes(lower, lower->dom.nz - 2, lo_top, &b)) != LBM_OK ||
+            (rc = lbm_zslab_moment_planes(lower, lower->dom.nz - 1, lo_ghost, &b)) != LBM_OK ||
+            (rc = lbm_zslab_moment_planes(upper, 0, up_ghost, &b)) != LBM_OK ||
+            (rc = lbm_zslab_moment_planes(upper, 1, up_bot, &b)) != LBM_OK)
+            return rc;
+        const cudaStream_t st = static_cast<cudaStream_t>(stream);
+        for (int c = 0; c < 10; ++c) {
+            CK(cudaMemcpyAsync(up_ghost[c], lo_top[c], (size_t)b, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(lo_ghost[c], up_bot[c], (size_t)b, cudaMemcpyDeviceToDevice, st));
+        }
+        return LBM_OK;
     }
     void *lo_top[5], *lo_ghost[5], *up_ghost[5], *up_bot[5];
     int64_t b = 0;
@@ -759,6 +806,10 @@ int lbm_zslab_plan_create(lbm_solver* const* slabs, int32_t n, lbm_zslab_plan** 
             a->storage != slabs[0]->storage) {
             set_error("lbm_zslab_plan_create: needs z-slab solvers of one x-y size and storage");
             return LBM_ERR_INVALID;
+        }
+        if (!is_aa(a)) {
+            set_error("lbm_zslab_plan_create: Legacy/Hybrid slabs only (HOME uses lbm_zslab_exchange)");
+            return LBM_ERR_UNSUPPORTED;
         }
     }
     const int64_t pl = (int64_t)slabs[0]->dom.nx * slabs[0]->dom.ny;

@@ -260,7 +260,10 @@ __device__ __forceinline__ void build(const Ring& R, int pos, int dir, const Coe
     }
 }
 
-template <class T, bool STATS, class IDX>
+// SLAB: the planes [p.zb, p.ze) of a z-slab and salts offset by p.salt_base;
+// otherwise every plane (a separate instantiation: the plain step is at its
+// register limit, and the two run-time bounds alone cost it spills)
+template <class T, bool STATS, class IDX, bool SLAB>
 __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
     extern __shared__ float sm[];
     const T* __restrict__ m = static_cast<const T*>(p.m);
@@ -275,8 +278,9 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
     int b = blockIdx.x;
     const int x0 = (b % tiles_x) * TX; b /= tiles_x;
     const int y0 = (b % tiles_y) * TY; b /= tiles_y;
-    const int z0 = b * p.zchunk;
-    const int z1 = min(nz, z0 + p.zchunk);
+    const int z0 = (SLAB ? p.zb : 0) + b * p.zchunk;
+    const int z1 = min(SLAB ? p.ze : nz, z0 + p.zchunk);
+    const uint32_t salt0 = SLAB ? p.salt_base : 0u;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     // this thread's position in the (TX+2) x (TY+2) halo tile, and its role
@@ -393,7 +397,8 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
             if (fcur & F_SOLID) {
 #pragma unroll
                 for (int c = 0; c < 10; ++c)
-                    MomStore<T>::st(op + (IDX)c * N, c, r0, c == 0 ? 1.f : 0.f, (uint32_t)id * 10u + c);
+                    MomStore<T>::st(op + (IDX)c * N, c, r0, c == 0 ? 1.f : 0.f,
+                                    ((uint32_t)id + salt0) * 10u + c);
             } else {
                 const Ring Rm(sm, z - 1), Rz(sm, z), Rp(sm, z + 1);
                 float fq[19];
@@ -430,7 +435,7 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
                                        Mxx - fmaf(rx, ux, r3), Mxy - rx * uy, Mxz - rx * uz,
                                        Myy - fmaf(ry, uy, r3), Myz - ry * uz, Mzz - fmaf(rz, uz, r3)};
 #pragma unroll
-                store_moments<T, IDX>(op, N, r0, out, (uint32_t)id);
+                store_moments<T, IDX>(op, N, r0, out, (uint32_t)id + salt0);
                 if (STATS) {
                     acc[0] += (double)r;
                     acc[1] += 0.5 * ((double)ux * ux + (double)uy * uy + (double)uz * uz);
@@ -466,11 +471,17 @@ __global__ void home_macros(const T* __restrict__ m, int64_t N, float r0, float*
 
 template <class T, bool STATS>
 void launch_step(const HomeParams& p, cudaStream_t s) {
-    const int grid = home_num_blocks(p.nx, p.ny, p.nz, p.zchunk);
+    const int grid = home_num_blocks(p.nx, p.ny, p.ze - p.zb, p.zchunk);
     const size_t smem = sizeof(float) * SMEM_FLOATS;
     // 32-bit element offsets while every index 10*N fits in them
-    if ((uint64_t)p.N * 10u < (1ull << 32)) home_step<T, STATS, uint32_t><<<grid, NT, smem, s>>>(p);
-    else home_step<T, STATS, int64_t><<<grid, NT, smem, s>>>(p);
+    const bool slab = p.zb != 0 || p.ze != p.nz || p.salt_base != 0;
+    if ((uint64_t)p.N * 10u < (1ull << 32)) {
+        if (slab) home_step<T, STATS, uint32_t, true><<<grid, NT, smem, s>>>(p);
+        else home_step<T, STATS, uint32_t, false><<<grid, NT, smem, s>>>(p);
+    } else {
+        if (slab) home_step<T, STATS, int64_t, true><<<grid, NT, smem, s>>>(p);
+        else home_step<T, STATS, int64_t, false><<<grid, NT, smem, s>>>(p);
+    }
 }
 
 template <class T>
@@ -488,18 +499,23 @@ cudaError_t home_prepare() {
     auto set = [&](const void* fn) {
         if (e == cudaSuccess) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     };
-    set((const void*)home_step<float, false, uint32_t>);
-    set((const void*)home_step<float, true, uint32_t>);
-    set((const void*)home_step<__half, false, uint32_t>);
-    set((const void*)home_step<__half, true, uint32_t>);
-    set((const void*)home_step<__nv_bfloat16, false, uint32_t>);
-    set((const void*)home_step<__nv_bfloat16, true, uint32_t>);
-    set((const void*)home_step<float, false, int64_t>);
-    set((const void*)home_step<float, true, int64_t>);
-    set((const void*)home_step<__half, false, int64_t>);
-    set((const void*)home_step<__half, true, int64_t>);
-    set((const void*)home_step<__nv_bfloat16, false, int64_t>);
-    set((const void*)home_step<__nv_bfloat16, true, int64_t>);
+    auto all = [&](auto slab) {
+        constexpr bool S = decltype(slab)::value;
+        set((const void*)home_step<float, false, uint32_t, S>);
+        set((const void*)home_step<float, true, uint32_t, S>);
+        set((const void*)home_step<__half, false, uint32_t, S>);
+        set((const void*)home_step<__half, true, uint32_t, S>);
+        set((const void*)home_step<__nv_bfloat16, false, uint32_t, S>);
+        set((const void*)home_step<__nv_bfloat16, true, uint32_t, S>);
+        set((const void*)home_step<float, false, int64_t, S>);
+        set((const void*)home_step<float, true, int64_t, S>);
+        set((const void*)home_step<__half, false, int64_t, S>);
+        set((const void*)home_step<__half, true, int64_t, S>);
+        set((const void*)home_step<__nv_bfloat16, false, int64_t, S>);
+        set((const void*)home_step<__nv_bfloat16, true, int64_t, S>);
+    };
+    all(std::false_type{});
+    all(std::true_type{});
     return e;
 }
 

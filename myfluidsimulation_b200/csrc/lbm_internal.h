@@ -50,6 +50,9 @@ struct HomeParams {
     int stats;
     int zchunk;              // planes per block
     int ref_bounce;          // 1: the reference's opposite table for reflections
+    int zb, ze;              // planes stepped: [zb, ze) (all, or a z-slab's interior)
+    uint32_t salt_base;      // added to a cell's index in the stochastic-rounding salt:
+                             // a slab passes its plane 0's index in the whole grid
 };
 
 // Launch configuration chosen by the host (autotuner or defaults).

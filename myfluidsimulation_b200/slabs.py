@@ -11,6 +11,11 @@ crossing each slab face (directions with c_z = +-1) travel twice:
 Nothing else is exchanged, and every cell computes exactly what it would in one
 grid, so a decomposed run equals the single-grid run bit for bit.
 
+HOME pulls whole planes of moments instead: before every step the 10 moment
+planes of each boundary plane go to the neighbour's ghost plane (phase 0 only),
+and each slab draws its stochastic-rounding bits by global cell index
+(`lbm_set_index_base`), so HOME slabs match the single grid bit for bit too.
+
 `SlabSet` keeps all slabs on one GPU, with device copies as the exchange.
 `DistSlab` keeps one slab per process (torch.distributed, NCCL between GPUs;
 any backend works for the plan), exchanging with point-to-point sends.
@@ -21,7 +26,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import BC_PERIODIC, METHOD_LEGACY, STORE_F32, check, lib
+from ._lib import BC_PERIODIC, METHOD_HOME, METHOD_LEGACY, STORE_F32, check, lib
 from .solvers import Solver
 
 __all__ = ["slab_bounds", "exchange_plan", "exchange", "with_ghosts", "SlabSet", "DistSlab"]
@@ -102,10 +107,12 @@ class SlabSet:
         self.stream = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         self.slabs = []
         self._plan = None
+        self.home = method == METHOD_HOME
         for z0, z1 in self.bounds:
             s = Solver(nx, ny, z1 - z0 + 2, tau, force, method=method, storage=storage, bc=bc, inlet_u=inlet_u,
                        stream=self.stream)
             check(lib().lbm_set_z_ghosts(s._h, 1))
+            check(lib().lbm_set_index_base(s._h, (z0 - 1) * nx * ny))
             self.slabs.append(s)
 
     def _drop_plan(self):
@@ -151,6 +158,9 @@ class SlabSet:
             self._plan = p
 
     def _exchange(self, phase):
+        if self.home:   # the moment planes move between buffers every step: per face
+            self.exchange_pairwise(phase)
+            return
         self._ensure_plan()
         check(lib().lbm_zslab_plan_exchange(self._plan, phase, C.c_void_p(self.stream)))
 
@@ -168,7 +178,8 @@ class SlabSet:
         import torch
         if n % 2 or n < 2:
             raise ValueError("n must be even")
-        self._ensure_plan()
+        if not self.home:
+            self._ensure_plan()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g, stream=torch.cuda.ExternalStream(self.stream)):
             self.step(n)
@@ -176,12 +187,12 @@ class SlabSet:
 
     def step(self, n: int = 1):
         for _ in range(n):
-            odd = _parity(self.slabs[0]) == 1
-            if odd:
+            ex = self.home or _parity(self.slabs[0]) == 1
+            if ex:
                 self._exchange(0)
             for s in self.slabs:
                 s.step(1)
-            if odd:
+            if ex and not self.home:
                 self._exchange(1)
 
     def synchronize(self):
@@ -193,7 +204,8 @@ class SlabSet:
         return tuple(np.concatenate([p[k][1:-1] for p in parts], axis=0) for k in range(4))
 
     def state(self):
-        """Populations of the whole grid in the natural layout (after an even step count)."""
+        """The whole grid's state: populations in the natural layout (after an even
+        step count), or HOME's 10 moments."""
         return np.concatenate([s.state()[:, 1:-1] for s in self.slabs], axis=1)
 
     def stats(self) -> dict:
@@ -241,21 +253,49 @@ class DistSlab:
         self.solver = Solver(nx, ny, self.z1 - self.z0 + 2, tau, force, method=method, storage=storage, bc=bc,
                              inlet_u=inlet_u, stream=torch.cuda.current_stream().cuda_stream)
         check(lib().lbm_set_z_ghosts(self.solver._h, 1))
+        check(lib().lbm_set_index_base(self.solver._h, (self.z0 - 1) * nx * ny))
+        self.home = method == METHOD_HOME
         L = self.z1 - self.z0 + 2
         planes = {"ghost_lo": 0, "first": 1, "last": L - 2, "ghost_hi": L - 1}
         self.planes = planes
         self.views = {}
-        for name, pl in planes.items():
-            for cz in (+1, -1):
-                ptrs, nb = _slot_ptrs(self.solver, pl, cz)
-                self.views[(name, cz)] = [_device_view(p, nb, self.device) for p in ptrs]
-        # phase 1 lands in staging first: only the values the neighbour's cells
-        # wrote are taken (lbm_zslab_merge), a bounced-back population stays
-        self.staging = {key: [torch.empty_like(t) for t in self.views[key]] for key in (("last", -1), ("first", 1))}
+        self._home_views = {}
+        if not self.home:
+            for name, pl in planes.items():
+                for cz in (+1, -1):
+                    ptrs, nb = _slot_ptrs(self.solver, pl, cz)
+                    self.views[(name, cz)] = [_device_view(p, nb, self.device) for p in ptrs]
+            # phase 1 lands in staging first: only the values the neighbour's cells
+            # wrote are taken (lbm_zslab_merge), a bounced-back population stays
+            self.staging = {key: [torch.empty_like(t) for t in self.views[key]]
+                            for key in (("last", -1), ("first", 1))}
+
+    def _moment_views(self):
+        """HOME: views of the 10 moment planes of each named plane in the current
+        buffer (the plan's direction sets both map to all 10 planes)."""
+        ptrs = {}
+        for name, pl in self.planes.items():
+            arr = (C.c_void_p * 10)()
+            nb = C.c_int64()
+            check(lib().lbm_zslab_moment_planes(self.solver._h, pl, arr, C.byref(nb)))
+            ptrs[name] = ([p for p in arr], nb.value)
+        key = tuple(ptrs["first"][0])
+        if key not in self._home_views:
+            v = {}
+            for name, (ps, nb) in ptrs.items():
+                ts = [_device_view(p, nb, self.device) for p in ps]
+                v[(name, 1)] = ts
+                v[(name, -1)] = ts
+            self._home_views[key] = v
+        return self._home_views[key]
 
     def _exchange(self, phase):
         if self.world == 1:
             check(lib().lbm_zslab_exchange(self.solver._h, self.solver._h, phase, C.c_void_p(self.solver.stream)))
+            return
+        if self.home:
+            if phase == 0:
+                exchange(self._moment_views(), 0, self.rank, self.world, self.dist, self.group)
             return
         if phase == 0:
             exchange(self.views, 0, self.rank, self.world, self.dist, self.group)
@@ -278,11 +318,11 @@ class DistSlab:
 
     def step(self, n: int = 1):
         for _ in range(n):
-            odd = _parity(self.solver) == 1
-            if odd:
+            ex = self.home or _parity(self.solver) == 1
+            if ex:
                 self._exchange(0)
             self.solver.step(1)
-            if odd:
+            if ex and not self.home:
                 self._exchange(1)
 
     def set_shear_omega(self, omega_s):

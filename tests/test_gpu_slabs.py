@@ -13,8 +13,8 @@ import numpy as np
 import pytest
 
 from myfluidsimulation_b200.slabs import SlabSet
-from myfluidsimulation_b200.solvers import (BC_DUCT, BC_PERIODIC, METHOD_HYBRID, METHOD_LEGACY, STORE_F16,
-                                            STORE_F32, Solver)
+from myfluidsimulation_b200.solvers import (BC_DUCT, BC_PERIODIC, METHOD_HOME, METHOD_HYBRID, METHOD_LEGACY,
+                                            STORE_BF16, STORE_F16, STORE_F32, Solver)
 
 pytestmark = pytest.mark.gpu
 
@@ -48,6 +48,10 @@ CASES = [
     ((40, 16, 18), 3, METHOD_LEGACY, STORE_F16, BC_PERIODIC),
     ((48, 18, 21), 3, METHOD_LEGACY, STORE_F32, BC_DUCT),
     ((17, 9, 12), 3, METHOD_LEGACY, STORE_F32, BC_PERIODIC),       # odd plane size: scalar even step
+    ((36, 20, 30), 3, METHOD_HOME, STORE_F32, BC_PERIODIC),
+    ((40, 16, 18), 4, METHOD_HOME, STORE_F16, BC_PERIODIC),         # stochastic rounding by global index
+    ((48, 18, 21), 2, METHOD_HOME, STORE_BF16, BC_DUCT),
+    ((36, 20, 30), 1, METHOD_HOME, STORE_F32, BC_PERIODIC),
 ]
 
 
@@ -82,11 +86,10 @@ def test_slabs_equal_single_grid(gpu, oracle, dims, parts, method, storage, bc):
 
 def test_slab_setter_rejects(gpu):
     from myfluidsimulation_b200 import lib
-    from myfluidsimulation_b200.solvers import BOUNCE_REFERENCE, METHOD_HOME
-    for kw in (dict(method=METHOD_HOME), dict(bounce=BOUNCE_REFERENCE)):
-        s = Solver(8, 8, 8, 0.6, **kw)
-        assert lib().lbm_set_z_ghosts(s._h, 1) != 0
-        s.close()
+    from myfluidsimulation_b200.solvers import BOUNCE_REFERENCE
+    s = Solver(8, 8, 8, 0.6, bounce=BOUNCE_REFERENCE)      # the two-buffer push form
+    assert lib().lbm_set_z_ghosts(s._h, 1) != 0
+    s.close()
     s = Solver(8, 8, 2, 0.6)
     assert lib().lbm_set_z_ghosts(s._h, 1) != 0
     s.close()
@@ -157,7 +160,7 @@ class _FakeDist:
         return [self._Work() for _ in ops]
 
 
-@pytest.mark.parametrize("world,method", [(2, METHOD_LEGACY), (3, METHOD_HYBRID)])
+@pytest.mark.parametrize("world,method", [(2, METHOD_LEGACY), (3, METHOD_HYBRID), (3, METHOD_HOME)])
 def test_dist_slabs_equal_single_grid(gpu, oracle, world, method):
     """DistSlab's multi-rank path (views of the slot planes, point-to-point plan,
     staging and merge) with `world` ranks emulated by threads on this GPU."""

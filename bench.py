@@ -193,8 +193,9 @@ def e2e_run(method, mask, args, torch):
     fields from pinned host memory, reinitialises from them, runs one drag
     interval and reads the macro fields and the statistics back.  The copies of
     consecutive steps are pipelined against the compute (lbm_stage_from_host /
-    lbm_reinit_from_stage / lbm_read_macros_async): the upload of step k+1 and
-    the read-back of step k run on the copy stream while step k+1 computes."""
+    lbm_reinit_from_stage / lbm_read_macros_async / lbm_get_stats_async): the
+    upload of step k+1 and the read-back of step k run while step k+1 computes,
+    and the timed region ends after the last read-back."""
     st = torch.cuda.current_stream()
     s, _ = make_solver(method, mask, st.cuda_stream)
     N = NX * NY * NZ
@@ -210,9 +211,11 @@ def e2e_run(method, mask, args, torch):
     from myfluidsimulation_b200._lib import check, lib
     L = lib()
     vp = lambda a: a.ctypes.data_as(C.c_void_p)
-    stats = np.zeros(8, np.float64)
+    stats = [torch.zeros(8, dtype=torch.float64, pin_memory=True).numpy() for _ in range(2)]
 
     def run(k_steps):
+        # every step's macro fields and statistics come back to pinned host
+        # buffers asynchronously; the loop waits for all of them at its end
         check(L.lbm_stage_from_host(s._h, vp(rho_h), vp(u_h), vp(v_h), vp(w_h)))
         for k in range(k_steps):
             check(L.lbm_reinit_from_stage(s._h))
@@ -220,8 +223,9 @@ def e2e_run(method, mask, args, torch):
                 check(L.lbm_stage_from_host(s._h, vp(rho_h), vp(u_h), vp(v_h), vp(w_h)))
             check(L.lbm_step(s._h, DRAG_EVERY))
             check(L.lbm_read_macros_async(s._h, *[vp(o) for o in outs[k % 2]]))
-            check(L.lbm_get_stats(s._h, vp(stats)))
+            check(L.lbm_get_stats_async(s._h, vp(stats[k % 2])))
         check(L.lbm_wait_reads(s._h))
+        check(L.lbm_synchronize(s._h))
 
     run(max(2, args.warmup // 2))
     torch.cuda.synchronize()

@@ -199,6 +199,12 @@ int lbm_enable_stats(lbm_solver* s, int enable);
  * computed them.  No reference counterpart (the reference sums on the host,
  * src/bench/main_taylor_green.cpp:157-182). */
 int lbm_get_stats(lbm_solver* s, double* out);
+/* The same copy without waiting: it is queued on the solver's copy stream
+ * after the steps queued so far (as lbm_read_macros_async is), and `out` (host
+ * memory, pinned for the copy to be asynchronous) holds their statistics once
+ * lbm_wait_reads or lbm_synchronize returns.  For loops that read every step's
+ * result without stalling the GPU on each one. */
+int lbm_get_stats_async(lbm_solver* s, double* out);
 
 /* Enables (1, the default) or disables (0) the macro-field output of
  * Legacy/Hybrid steps.  Disabled, lbm_step writes only the populations (the

@@ -96,6 +96,7 @@ _PROTOS = [
     ("lbm_step_count", C.c_int, [_P, C.POINTER(C.c_int64)]),
     ("lbm_enable_stats", C.c_int, [_P, C.c_int]),
     ("lbm_get_stats", C.c_int, [_P, _P]),
+    ("lbm_get_stats_async", C.c_int, [_P, _P]),
     ("lbm_set_macro_output", C.c_int, [_P, C.c_int]),
     ("lbm_macro_stats_static", C.c_int, [_P, _P, _P, _P, _P, C.c_int64, _P, _P]),
     ("lbm_batch_create", C.c_int, [C.POINTER(_P), C.c_int32, _P, C.POINTER(_P)]),

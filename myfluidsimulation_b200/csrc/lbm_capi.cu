@@ -969,6 +969,20 @@ int lbm_get_stats(lbm_solver* s, double* out) {
     return LBM_OK;
 }
 
+int lbm_get_stats_async(lbm_solver* s, double* out) {
+    if (!s || !out) { set_error("lbm_get_stats_async: null argument"); return LBM_ERR_INVALID; }
+    // on the copy stream, behind the macro read-back: a device-to-host copy on
+    // the solver's stream would wait for the copy engine and stall the steps
+    int rc = ensure_copy_path(s);
+    if (rc != LBM_OK) return rc;
+    CK(cudaEventRecord(s->ev_macros, s->stream));
+    CK(cudaStreamWaitEvent(s->copy_stream, s->ev_macros, 0));
+    CK(cudaMemcpyAsync(out, s->stats, sizeof(double) * lbm::NSTAT, cudaMemcpyDeviceToHost, s->copy_stream));
+    CK(cudaEventRecord(s->ev_read, s->copy_stream));
+    s->read_pending = true;   // the next step that writes statistics waits for this copy
+    return LBM_OK;
+}
+
 int lbm_voxelize(const float* tris, int64_t ntri, const float* bb_in, const lbm_voxel_params* p, uint8_t* mask_out) {
     if (!p || !mask_out || (ntri > 0 && !tris) || ntri < 0) { set_error("lbm_voxelize: bad argument"); return LBM_ERR_INVALID; }
     if (p->nx < 1 || p->ny < 1 || p->nz < 1) { set_error("lbm_voxelize: bad dimensions"); return LBM_ERR_INVALID; }

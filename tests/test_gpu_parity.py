@@ -357,3 +357,27 @@ def test_narrow_storage_vs_oracle(gpu, oracle, storage, tol, method, dims, bc):
     e_r = rl2(rho[fl] - 1.0, r_o[fl] - 1.0)
     print(f"storage {storage} method {method} dims {dims}: u rel L2 {e_u:.3e}, rho-1 rel L2 {e_r:.3e}")
     assert e_u < tol
+
+
+def test_stats_async_equals_sync(gpu):
+    """lbm_get_stats_async queues the same copy that lbm_get_stats waits for."""
+    import ctypes as C
+    import torch
+    from myfluidsimulation_b200 import lib
+    dims = (24, 16, 12)
+    s = Solver(*dims, 0.6, (1e-5, 0, 0))
+    s.set_solid_mask(obstacle_mask(*dims, seed=21))
+    s.reinit_from_host(*init_fields(*dims, seed=22))
+    s.enable_stats(True)
+    got = []
+    for k in range(3):
+        s.step(5)
+        buf = torch.zeros(8, dtype=torch.float64, pin_memory=True).numpy()
+        assert lib().lbm_get_stats_async(s._h, buf.ctypes.data_as(C.c_void_p)) == 0
+        got.append(buf)
+    s.synchronize()
+    final = s.stats()
+    np.testing.assert_array_equal(got[-1], np.array([final[k] for k in ("mass", "ke_sum", "drag_x", "drag_y", "drag_z",
+                                                                        "mom_x", "mom_y", "mom_z")]))
+    assert not np.array_equal(got[0], got[-1])
+    s.close()

@@ -63,6 +63,13 @@ struct Ring {
         mid = sm + MID_OFF + (p & 1) * MID_SZ;
         dn = sm + DN_OFF;
     }
+    // the same with the UP slot (p mod 3) given: the step loop rotates the
+    // three slots instead of dividing by 3 for every ring
+    __device__ __forceinline__ Ring(float* sm, int p, int upslot) {
+        up = sm + upslot * UP_SZ;
+        mid = sm + MID_OFF + (p & 1) * MID_SZ;
+        dn = sm + DN_OFF;
+    }
     template <int q>
     __device__ __forceinline__ float& at(int pos) const {
         return (cz(q) > 0 ? up : (cz(q) == 0 ? mid : dn))[gofs(q) + pos];
@@ -321,28 +328,30 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
     };
     // the moments of plane pz are in mreg/freg: write the populations leaving it
     // (a solid cell writes none; its slots are filled by its fluid neighbours)
-    auto arrive = [&](int pz) {
+    auto arrive = [&](int pz, int upslot) {
         if (exists && !(freg & F_SOLID)) {
             Coef<float> c;
             c.set(mreg, omw, r0);
-            build(Ring(sm, pz), pos, dir, c);
+            build(Ring(sm, pz, upslot), pos, dir, c);
         }
     };
+    auto mod3 = [](int v) { return v < 0 ? v + 3 : v % 3; };   // v >= -1
+    int um = mod3(z0 - 1), u0 = mod3(z0), up = mod3(z0 + 1);  // UP slots of planes z-1, z, z+1
 
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
 
     load(z0 - 1);
-    arrive(z0 - 1);
+    arrive(z0 - 1, um);
     load(z0);
-    arrive(z0);
+    arrive(z0, u0);
     uint32_t fcur = freg;          // this position's flags in the plane being gathered
     load(z0 + 1);
 
     for (int z = z0; z < z1; ++z) {
         // 1. plane z+1 arrives (its moments were loaded one iteration ago); z+2 is requested
-        arrive(z + 1);
+        arrive(z + 1, up);
         const uint32_t fnext = freg;
         if (z + 2 <= z1) load(z + 2);
         // 2. a link that does not stream: the cell writes the replacement into the
@@ -355,7 +364,7 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
             for (int c = 0; c < 10; ++c) own[c] = MomStore<T>::ld(m + (IDX)c * N + id, c, r0);
             Coef<float> oc;
             oc.set(own, omw, r0);
-            const Ring Rm(sm, z - 1), Rz(sm, z), Rp(sm, z + 1);
+            const Ring Rm(sm, z - 1, um), Rz(sm, z, u0), Rp(sm, z + 1, up);
             static_for<1, 19>([&](auto qi) {
                 constexpr int q = decltype(qi)::value;
                 if ((lk >> opp(q)) & 1u) {
@@ -400,7 +409,7 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
                     MomStore<T>::st(op + (IDX)c * N, c, r0, c == 0 ? 1.f : 0.f,
                                     ((uint32_t)id + salt0) * 10u + c);
             } else {
-                const Ring Rm(sm, z - 1), Rz(sm, z), Rp(sm, z + 1);
+                const Ring Rm(sm, z - 1, um), Rz(sm, z, u0), Rp(sm, z + 1, up);
                 float fq[19];
                 static_for<0, 19>([&](auto qi) {
                     constexpr int q = decltype(qi)::value;
@@ -446,6 +455,12 @@ __global__ void __launch_bounds__(NT, 3) home_step(HomeParams p) {
             }
         }
         fcur = fnext;
+        {   // plane z+2 takes the slot of plane z-1
+            const int t = um;
+            um = u0;
+            u0 = up;
+            up = t;
+        }
         __syncthreads();
     }
     if constexpr (STATS) block_reduce_stats(acc, p.partials);

@@ -359,6 +359,40 @@ def test_narrow_storage_vs_oracle(gpu, oracle, storage, tol, method, dims, bc):
     assert e_u < tol
 
 
+@pytest.mark.parametrize("storage,tol", [(1, 2e-3), (2, 2e-2)])
+@pytest.mark.parametrize("dims", [(64, 12, 10), (128, 8, 6), (192, 5, 4)])
+def test_narrow_periodic_vs_oracle(gpu, oracle, storage, tol, dims):
+    """F16/BF16 on periodic grids without solid cells (the 512^3 TGV's case):
+    odd and even step counts, forces on all three axes, against the FP64 oracle
+    and against the FP32 run (the error stays at the storage's rounding level)."""
+    nx, ny, nz = dims
+    fields = init_fields(*dims, seed=31)
+    frc = (1e-5, -2e-6, 3e-6)
+    for steps in (1, 8):
+        s = Solver(nx, ny, nz, 0.6, frc, storage=storage)
+        s.reinit_from_host(*fields)
+        s.enable_stats(True)
+        s.step(steps)
+        s.synchronize()
+        rho, u, v, w = s.macros()
+        st = s.stats()
+        s.close()
+        ref = Solver(nx, ny, nz, 0.6, frc)
+        ref.reinit_from_host(*fields)
+        ref.enable_stats(True)
+        ref.step(steps)
+        ref.synchronize()
+        r32 = ref.macros()
+        st32 = ref.stats()
+        ref.close()
+        _, r_o, u_o, v_o, w_o, _ = oracle.bgk_run(oracle.reinit_eq(*fields), None, steps, 0.6, frc)
+        e_u = vel_err([u, v, w], [u_o, v_o, w_o])
+        e_32 = vel_err([u, v, w], list(r32[1:]))
+        print(f"storage {storage} dims {dims} steps {steps}: u rel L2 {e_u:.3e} (vs FP32 {e_32:.3e})")
+        assert e_u < tol and e_32 < tol
+        assert abs(st["mass"] - st32["mass"]) <= 1e-4 * abs(st32["mass"])
+
+
 def test_stats_async_equals_sync(gpu):
     """lbm_get_stats_async queues the same copy that lbm_get_stats waits for."""
     import ctypes as C

@@ -1,29 +1,37 @@
 #!/usr/bin/env python
-"""D3Q19 MLUPS and HBM-roofline fraction on the duct-past-a-sphere workload.
+"""D3Q19 MLUPS and HBM-roofline fraction on the duct-past-a-sphere workloads.
 
-Workload (one bench step = one drag interval): a 256x128x128 duct, velocity
-inlet u=0.05 at x=0, zero-gradient outlet, halfway bounce-back walls on the
-y/z faces, tau=0.56, flow past an icosphere (5,120 triangles, radius 16
-cells, centre (64,64,64)) voxelized on the GPU; 50 LBM steps with the
-momentum-exchange drag recorded at the last one.  Inputs are synthetic
-(generated from fixed parameters; no dataset).  The state (319 MB of FP32
-populations) is larger than L2, so no flush is needed between steps.
+Two workloads share one grid and one solid mask: a 256x128x128 duct with
+solid wall cells on its y/z faces and an icosphere (5,120 triangles, radius
+16 cells, centre (64,64,64)) voxelized by ray parity, tau = 0.56.
+  * "periodic": x periodic, driven by a body force (1e-5, 0, 0), started
+    from rho = 1, u = 0.  This is the form the reference's own solvers can
+    run (they have no inlet/outlet), so both arms time the same work.
+  * "inlet": uniform velocity inlet u = 0.05 at x = 0, zero-gradient outflow
+    at x = 255, started from rho = 1, u = 0.05.
+One bench step = 50 LBM steps (one drag interval) with the FP64 statistics
+(mass, energy, momentum, momentum-exchange drag) taken at the last one.
+Inputs are synthetic (generated from fixed parameters; no dataset).  The
+state (319 MB of FP32 populations) is larger than L2, so no flush is needed
+between steps.
 
-`value` is Legacy BGK FP32 (the fluidsim_legacy path); HOME and Hybrid(B0=2)
-are measured on the same workload and reported under "methods".
+`value` is Legacy BGK FP32 on the periodic workload; every method on both
+workloads is reported under "methods" (keys `legacy`, `home`, `hybrid` for the
+periodic workload, `*_inlet` for the inlet duct).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 With --gpus N (under torchrun) every rank runs its own duct instance (weak
 scaling, no data-path collective); time is the max over ranks.
---impl reference times the reference's own CUDA build (compiled from its
-sources into oracle/_ref) on the closest workload it supports: the same grid,
-mask and tau with the duct walls as solid cells, periodic in x and driven by
-a body force, because the reference has no inlet/outlet boundary.
+--impl reference times the reference's own CUDA solvers (compiled from its
+sources into oracle/_ref) on the periodic workload, Legacy, HOME and
+Hybrid(B0=2), with the mask built by the reference's own STL loader and
+voxelizer (oracle/_ref/libref_cpu.so); it loads nothing of this library.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import math
 import os
@@ -43,12 +51,41 @@ sys.path.insert(0, ROOT)
 NX, NY, NZ = 256, 128, 128
 TAU = 0.56
 U_IN = 0.05
+FORCE = (1e-5, 0.0, 0.0)
 DRAG_EVERY = 50
 RADIUS, CENTER = 16, (64, 64, 64)
 B0 = 2
 # algorithmic bytes per cell-update (state read once + written once, plus the mask/flag byte)
 BYTES = {"legacy": 19 * 4 * 2 + 1, "hybrid": 19 * 4 * 2 + 1, "home": 10 * 4 * 2 + 1}
 KERNEL = {"legacy": "aa_even/aa_odd", "hybrid": "aa_even/aa_odd", "home": "home_step"}
+METRIC = "D3Q19 MLUPS (Legacy BGK FP32, duct 256x128x128 past a voxelized sphere)"
+WORKLOAD_TEXT = {
+    "periodic": "duct 256x128x128, y/z walls as solid cells, icosphere (5120 triangles, r=16, centre (64,64,64)) "
+                "voxelized by ray parity, x periodic, body force (1e-5,0,0), tau 0.56, start rho=1 u=0; "
+                "one step = 50 LBM steps + FP64 statistics",
+    "inlet": "duct 256x128x128, inlet u=0.05 at x=0, zero-gradient outflow, y/z walls as solid cells, icosphere "
+             "(5120 triangles, r=16) voxelized by ray parity, tau 0.56, start rho=1 u=0.05; one step = 50 LBM "
+             "steps + FP64 statistics (drag)",
+}
+# the configuration both arms print for the headline (Legacy, periodic workload)
+HEAD_CONFIG = {"workload": WORKLOAD_TEXT["periodic"], "method": "legacy", "storage": "f32",
+               "l2": "state larger than L2 (no flush needed)"}
+RUNS = [("legacy", "periodic"), ("home", "periodic"), ("hybrid", "periodic"),
+        ("legacy", "inlet"), ("home", "inlet"), ("hybrid", "inlet")]
+
+
+def run_key(method, workload):
+    return method if workload == "periodic" else f"{method}_inlet"
+
+
+def load_workloads():
+    """The input generator (pure numpy), loaded from its file so that nothing of
+    the library's package (and no native code) is imported with it."""
+    spec = importlib.util.spec_from_file_location(
+        "_bench_workloads", os.path.join(ROOT, "myfluidsimulation_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def measured_peaks():
@@ -119,9 +156,9 @@ class ClockSampler:
 
 
 def build_mask(tmpdir):
-    """Icosphere STL -> library loader -> GPU voxelizer -> duct walls."""
+    """Icosphere STL -> the library's STL loader -> its GPU voxelizer -> duct walls."""
     from myfluidsimulation_b200 import geometry as G
-    from myfluidsimulation_b200 import workloads as W
+    W = load_workloads()
     tris, scale, tr = W.duct_sphere_mesh(NX, NY, NZ, RADIUS, CENTER)
     path = os.path.join(tmpdir, "icosphere.stl")
     W.write_binary_stl(path, tris)
@@ -130,27 +167,60 @@ def build_mask(tmpdir):
     return W.duct_mask(NX, NY, NZ, sphere), int(mesh.tris.shape[0]), int(sphere.sum())
 
 
-def make_solver(method, mask, stream):
-    from myfluidsimulation_b200.solvers import BC_DUCT, METHOD_HOME, METHOD_HYBRID, METHOD_LEGACY, Solver
+def initial_fields(workload, mask):
+    rho = np.ones((NZ, NY, NX), np.float32)
+    u = np.full((NZ, NY, NX), U_IN if workload == "inlet" else 0.0, np.float32)
+    u[mask != 0] = 0
+    return rho, u
+
+
+def make_solver(method, workload, mask, stream):
+    from myfluidsimulation_b200.solvers import (BC_DUCT, BC_PERIODIC, METHOD_HOME, METHOD_HYBRID, METHOD_LEGACY,
+                                                Solver)
     m = {"legacy": METHOD_LEGACY, "home": METHOD_HOME, "hybrid": METHOD_HYBRID}[method]
-    s = Solver(NX, NY, NZ, TAU, method=m, bc=BC_DUCT, inlet_u=U_IN, stream=stream)
+    if workload == "inlet":
+        s = Solver(NX, NY, NZ, TAU, method=m, bc=BC_DUCT, inlet_u=U_IN, stream=stream)
+    else:
+        s = Solver(NX, NY, NZ, TAU, FORCE, method=m, bc=BC_PERIODIC, stream=stream)
     s.set_solid_mask(mask)
     nb = s.build_band(B0) if method == "hybrid" else 0
-    rho = np.ones((NZ, NY, NX), np.float32)
-    u = np.full((NZ, NY, NX), U_IN, np.float32)
-    u[mask != 0] = 0
+    rho, u = initial_fields(workload, mask)
     s.reinit_from_host(rho, u, None, None)
     s.enable_stats(True)
     return s, nb
 
 
-def run_method(method, mask, args, torch, rank):
+def kernel_split(s, method, torch, launches=40):
+    """Per-kernel device time: single-substep launches (no macro fields, no
+    statistics) queued back to back with a CUDA event between every two, no
+    synchronisation inside the loop.  Returns {kernel: median us}."""
     st = torch.cuda.current_stream()
-    s, nb = make_solver(method, mask, st.cuda_stream)
+    s.enable_stats(False)
+    s.set_macro_output(False)
+    s.step(2)
+    par = s.steps % 2                  # parity of the first timed launch (AA)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(launches + 1)]
+    ev[0].record(st)
+    for i in range(launches):
+        s.step(1)
+        ev[i + 1].record(st)
+    torch.cuda.synchronize()
+    t = [1e3 * ev[i].elapsed_time(ev[i + 1]) for i in range(launches)]
+    s.set_macro_output(True)
+    s.enable_stats(True)
+    if method == "home":
+        return {"home_step": round(statistics.median(t), 2)}
+    a, b = t[0::2], t[1::2]
+    names = ("aa_even", "aa_odd") if par == 0 else ("aa_odd", "aa_even")
+    return {names[0]: round(statistics.median(a), 2), names[1]: round(statistics.median(b), 2)}
+
+
+def run_method(method, workload, mask, args, torch):
+    st = torch.cuda.current_stream()
+    s, nb = make_solver(method, workload, mask, st.cuda_stream)
     for _ in range(args.warmup):
         s.step(DRAG_EVERY)
     torch.cuda.synchronize()
-    drags = []
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(st)
@@ -160,35 +230,13 @@ def run_method(method, mask, args, torch, rank):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     st_ = s.stats()
-    drags.append([st_["drag_x"], st_["drag_y"], st_["drag_z"]])
     res = {"ms_total": ms, "launches": args.steps * (DRAG_EVERY + 1), "band_cells": nb,
-           "drag_last": drags[-1], "mass": st_["mass"]}
-    # per-kernel split (outside the timed region): single steps, no macro/stats output,
-    # CUDA events around each launch; Legacy/Hybrid alternate the even and odd kernels
-    s.enable_stats(False)
-    s.set_macro_output(False)
-    split = [[], []]
-    for i in range(20):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(st)
-        s.step(1)
-        b.record(st)
-        torch.cuda.synchronize()
-        split[i % 2].append(a.elapsed_time(b))
-    s.set_macro_output(True)
-    s.enable_stats(True)
-    par = (args.warmup + args.steps) * DRAG_EVERY % 2      # parity of the first split launch
-    if method == "home":
-        res["kernel_us"] = {"home_step": round(1e3 * statistics.median(split[0] + split[1]), 2)}
-    else:
-        names = ("aa_even", "aa_odd") if par == 0 else ("aa_odd", "aa_even")
-        res["kernel_us"] = {names[0]: round(1e3 * statistics.median(split[0]), 2),
-                            names[1]: round(1e3 * statistics.median(split[1]), 2)}
+           "drag_last": [st_["drag_x"], st_["drag_y"], st_["drag_z"]], "mass": st_["mass"],
+           "kernel_us": kernel_split(s, method, torch)}
     return s, res
 
 
-def e2e_run(method, mask, args, torch):
+def e2e_run(method, workload, mask, args, torch):
     """Through the public C-ABI with host buffers: every step uploads the macro
     fields from pinned host memory, reinitialises from them, runs one drag
     interval and reads the macro fields and the statistics back.  The copies of
@@ -197,13 +245,13 @@ def e2e_run(method, mask, args, torch):
     upload of step k+1 and the read-back of step k run while step k+1 computes,
     and the timed region ends after the last read-back."""
     st = torch.cuda.current_stream()
-    s, _ = make_solver(method, mask, st.cuda_stream)
+    s, _ = make_solver(method, workload, mask, st.cuda_stream)
     N = NX * NY * NZ
     pin = lambda: torch.empty(N, dtype=torch.float32, pin_memory=True).numpy().reshape(NZ, NY, NX)
     rho_h, u_h, v_h, w_h = pin(), pin(), pin(), pin()
-    rho_h[:] = 1.0
-    u_h[:] = U_IN
-    u_h[mask != 0] = 0
+    r0, u0 = initial_fields(workload, mask)
+    rho_h[:] = r0
+    u_h[:] = u0
     v_h[:] = 0
     w_h[:] = 0
     outs = [[pin() for _ in range(4)] for _ in range(2)]
@@ -246,81 +294,105 @@ def e2e_run(method, mask, args, torch):
 
 def cpu_baseline(mask, gpu_state_fn):
     """The FP64 oracle (the C restatement, OpenMP over the host cores) on a bounded
-    sample of the same workload: the full grid for a few steps."""
+    sample of the headline workload: the full grid for a few steps."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_bind import Oracle
     o = Oracle()
     nthreads = o.lib.orc_num_threads()
     rho = np.ones((NZ, NY, NX))
-    u = np.full((NZ, NY, NX), np.float64(np.float32(U_IN)))
-    u[mask != 0] = 0
+    u = np.zeros((NZ, NY, NX))
     f0 = o.reinit_eq(rho, u, None, None)
+    force = tuple(float(np.float32(x)) for x in FORCE)
     # size the sample to ~10-20 s: time one step first
     t = time.perf_counter()
-    o.bgk_run(f0, mask, 1, TAU, bc=1, u_in=np.float32(U_IN))
+    o.bgk_run(f0, mask, 1, TAU, force=force)
     t1 = time.perf_counter() - t
     steps = int(max(2, min(40, 12.0 / max(t1, 1e-3))))
     t = time.perf_counter()
-    f, r, ux, uy, uz, drag = o.bgk_run(f0, mask, steps, TAU, bc=1, u_in=np.float32(U_IN))
+    f, r, ux, uy, uz, drag = o.bgk_run(f0, mask, steps, TAU, force=force)
     dt = time.perf_counter() - t
     mlups = NX * NY * NZ * steps / dt / 1e6
     # the same sample on the GPU: relative L2 of the state against FP64
     g = gpu_state_fn(steps)
     err = float(np.linalg.norm(g - f) / np.linalg.norm(f))
     return {"value": round(mlups, 2), "unit": "MLUPS", "cores": int(nthreads), "kind": "port",
-            "sample": f"FP64 oracle (C, OpenMP) Legacy BGK duct {NX}x{NY}x{NZ}, {steps} steps"}, err, steps
+            "sample": f"FP64 oracle (C, OpenMP) Legacy BGK, periodic duct {NX}x{NY}x{NZ}, {steps} steps"}, err, steps
+
+
+def reference_mask(tmpdir):
+    """The duct mask built by the reference's own code (oracle/_ref/libref_cpu.so:
+    its stl_loader.cpp and voxelize.cpp) from the same generated icosphere."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_bind import RefCPU
+    W = load_workloads()
+    tris, scale, tr = W.duct_sphere_mesh(NX, NY, NZ, RADIUS, CENTER)
+    path = os.path.join(tmpdir, "icosphere.stl")
+    W.write_binary_stl(path, tris)
+    R = RefCPU()
+    t, bb = R.load_stl(path)
+    sphere = R.voxelize(t, bb, (NX, NY, NZ), scale, tr)
+    return W.duct_mask(NX, NY, NZ, sphere), R
 
 
 def reference_arm(args, torch, rank, world):
-    """The reference's own CUDA build on the same grid/mask/tau, force-driven periodic duct."""
+    """The reference's own CUDA solvers on the periodic workload: Legacy (the
+    headline), HOME and Hybrid(B0=2), each timed over `steps` calls of step(50)
+    with cudaEvents on the default stream, as its own sweep times them
+    (src/main_compare.cpp:539-553).  Nothing of this library is loaded."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from oracle_bind import RefCUDA
-    base = {"metric": "D3Q19 MLUPS (Legacy BGK FP32, duct 256x128x128 past a voxelized sphere)", "unit": "MLUPS",
-            "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
-    if not RefCUDA.available():
+    from oracle_bind import RefCPU, RefCUDA
+    base = {"metric": METRIC, "unit": "MLUPS", "impl": "reference", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic"}
+    if not (RefCUDA.available() and RefCPU.available()):
         if rank == 0:
-            base.update({"unavailable": "reference CUDA build oracle/_ref/libref_cuda.so not present"})
+            base["unavailable"] = "the reference's build oracle/_ref/libref_cuda.so / libref_cpu.so is not present"
             print(json.dumps(base))
         return
     if rank != 0:
         return
     with tempfile.TemporaryDirectory() as td:
-        mask, ntri, nsph = build_mask(td)
+        mask, RC = reference_mask(td)
+    solid = (mask != 0).astype(np.uint8)
     R = RefCUDA()
-    h = R.create(0, (NX, NY, NZ), TAU, (1e-5, 0.0, 0.0))
-    R.set_mask(h, (mask != 0).astype(np.uint8))
-    R.init_rho(h, None)
-    R.time_steps(h, args.warmup, DRAG_EVERY)
-    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
-        ms = R.time_steps(h, args.steps, DRAG_EVERY)
-    R.destroy(h)
     N = NX * NY * NZ
-    mlups = N * DRAG_EVERY * args.steps / (ms * 1e-3) / 1e6
+    methods = {}
+    clocks = None
+    for name, mid in (("legacy", 0), ("home", 1), ("hybrid", 2)):
+        h = R.create(mid, (NX, NY, NZ), TAU, FORCE)
+        R.set_mask(h, solid)
+        if name == "hybrid":
+            _, leg = RC.band(solid, B0)        # the reference's own band BFS (sim_runner.hpp)
+            R.set_legacy(h, leg)
+        R.init_rho(h, None)                    # rho = 1, u = 0 (sim_runner.hpp:135-137)
+        R.time_steps(h, args.warmup, DRAG_EVERY)
+        if name == "legacy":
+            with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+                ms = R.time_steps(h, args.steps, DRAG_EVERY)
+            clocks = clk.summary()
+        else:
+            ms = R.time_steps(h, args.steps, DRAG_EVERY)
+        R.destroy(h)
+        mlups = N * DRAG_EVERY * args.steps / (ms * 1e-3) / 1e6
+        methods[name] = {"mlups": round(mlups, 1), "ms_per_step": round(ms / args.steps, 4),
+                         "call": {"legacy": "LBM3D_Legacy::step(50)", "home": "LBM3D_Home::step(50)",
+                                  "hybrid": "LBM3D_Hybrid::step(50)"}[name]}
+    h = methods["legacy"]
     base.update({
-        "value": round(mlups, 1), "ms_per_step": round(ms / args.steps, 4),
-        "config": {"workload": "duct 256x128x128, icosphere r=16 mask, tau 0.56, walls as solid cells, "
-                               "x periodic, body force 1e-5 (the reference has no inlet/outlet)",
-                   "method": "LBM3D_Legacy::step(50) of the reference build", "l2": "state 637 MB > L2"},
-        "cpu_baseline": {"value": round(mlups, 1), "unit": "MLUPS", "cores": 0, "kind": "reference",
-                         "device": "cuda:0",
-                         "sample": f"reference CUDA build (oracle/_ref/libref_cuda.so), {args.steps}x50 steps"},
-        "e2e": {"value": round(mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "clocks": clk.summary(),
+        "value": h["mlups"], "ms_per_step": h["ms_per_step"], "config": dict(HEAD_CONFIG),
+        "methods": methods,
+        "cpu_baseline": {"value": h["mlups"], "unit": "MLUPS", "cores": 0, "kind": "reference", "device": "cuda:0",
+                         "sample": f"the reference's CUDA solvers (oracle/_ref/libref_cuda.so), {args.steps} x 50 "
+                                   "steps per method; mask from its own STL loader and voxelizer"},
+        "e2e": {"value": h["mlups"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clocks,
     })
     print(json.dumps(base))
 
 
-def precision_study(args, torch):
-    """512^3 periodic Taylor-Green vortex (tau 0.51, u0 0.05, k 2pi/512): MLUPS of
-    FP32 / F16 / BF16 storage for Legacy and HOME, and the kinetic-energy decay
-    of each form against the FP32 run of the same method after --tgv-steps steps."""
-    from myfluidsimulation_b200.solvers import METHOD_HOME, METHOD_LEGACY, STORE_BF16, STORE_F16, STORE_F32, Solver
-    n = args.tgv_n
-    N = n ** 3
-    steps = args.tgv_steps
-    st = torch.cuda.current_stream()
-    # the analytic field at cell centres, built on the device in FP64 and cast
+def tgv_fields(n, torch):
+    """The 3-D Taylor-Green field of n^3 cells (u0 0.05, k 2 pi / n) at cell
+    centres, built on the device in FP64 and cast to FP32: rho, u, v, w."""
     k = 2 * math.pi / n
     c = (torch.arange(n, device="cuda", dtype=torch.float64) + 0.5) * k
     z, y, x = c.view(n, 1, 1), c.view(1, n, 1), c.view(1, 1, n)
@@ -328,14 +400,50 @@ def precision_study(args, torch):
     v = (-0.05 * torch.cos(x) * torch.sin(y) * torch.cos(z)).float().contiguous()
     w = torch.zeros_like(u)
     rho = (1.0 + 3.0 * (0.05 ** 2 / 16.0) * (torch.cos(2 * x) + torch.cos(2 * y)) * (torch.cos(2 * z) + 2.0)).float().contiguous()
-    del c, z, y, x
+    return rho, u, v, w
+
+
+def _device_field(ptr, n, torch):
+    """A float32 torch view of n values of device memory (no copy)."""
+    class _Mem:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<f4", "data": (int(ptr), False), "version": 3,
+                                    "strides": None}
+    return torch.as_tensor(_Mem(), device="cuda")
+
+
+def _rel_l2(a, b):
+    d = (a.double() - b.double()).norm().item()
+    return d / max(b.double().norm().item(), 1e-300)
+
+
+def precision_study(args, torch):
+    """512^3 periodic Taylor-Green vortex (tau 0.51, u0 0.05, k 2pi/512), Legacy and
+    HOME, in FP64 (storage and arithmetic: the reference form), FP32, F16 and BF16:
+      * MLUPS over --steps steps after 4 warm-up steps (CUDA events, macro output
+        off), with the roofline fraction of the algorithmic bytes, and the
+        even/odd launch split (events between back-to-back launches);
+      * from the initial field, the kinetic energy (FP64 reduction on the GPU)
+        every --tgv-every steps up to --tgv-steps, and the fields at the end;
+      * every form's energy curve (max relative error over the samples) and
+        final fields (relative L2 of rho - 1 and of u) against the FP64 run of
+        the same method.
+    The reference's own HOME (FP32, oracle/_ref/libref_cuda.so) runs the same
+    case for its time and error; its Legacy cannot (its int32 indices overflow
+    above about 483^3 cells)."""
+    from myfluidsimulation_b200.solvers import (METHOD_HOME, METHOD_LEGACY, STORE_BF16, STORE_F16, STORE_F32,
+                                                STORE_F64, Solver)
+    n = args.tgv_n
+    N = n ** 3
+    steps, every = args.tgv_steps, args.tgv_every
+    st = torch.cuda.current_stream()
+    rho, u, v, w = tgv_fields(n, torch)
     out = {}
-    bytes_cell = {("legacy", STORE_F32): 152, ("legacy", STORE_F16): 76, ("legacy", STORE_BF16): 76,
-                  ("home", STORE_F32): 80, ("home", STORE_F16): 40, ("home", STORE_BF16): 40}
-    peak, _ = measured_peaks()
-    for mname, m in (("legacy", METHOD_LEGACY), ("home", METHOD_HOME)):
-        ref_ke = None
-        for sname, sto in (("f32", STORE_F32), ("f16", STORE_F16), ("bf16", STORE_BF16)):
+    forms = (("f64", STORE_F64, 8), ("f32", STORE_F32, 4), ("f16", STORE_F16, 2), ("bf16", STORE_BF16, 2))
+    peak, peak_kind = measured_peaks()
+    ref_fields, ref_ke_end = {}, {}
+    for mname, m, ncomp in (("legacy", METHOD_LEGACY, 19), ("home", METHOD_HOME, 10)):
+        ref_curve = None
+        for sname, sto, esz in forms:
             s = Solver(n, n, n, 0.51, method=m, storage=sto, stream=st.cuda_stream)
             s.reinit_from_macro(rho, u, v, w)
             s.set_macro_output(False)
@@ -351,35 +459,76 @@ def precision_study(args, torch):
             ms = e0.elapsed_time(e1)
             mlups = N * args.steps / (ms * 1e-3) / 1e6
             # per-launch split: Legacy alternates the local (even) and neighbour (odd) kernels
-            split = [[], []]
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(9)]
+            ev[0].record(st)
             for i in range(8):
-                a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a_.record(st)
                 s.step(1)
-                b_.record(st)
-                torch.cuda.synchronize()
-                split[i % 2].append(a_.elapsed_time(b_) * 1e3)
+                ev[i + 1].record(st)
+            torch.cuda.synchronize()
+            t = [1e3 * ev[i].elapsed_time(ev[i + 1]) for i in range(8)]
             # accuracy run from the initial field
             s.reinit_from_macro(rho, u, v, w)
+            s.set_macro_output(True)
             s.enable_stats(True)
-            s.step(1)
-            ke0 = s.stats()["ke_sum"] / N
-            s.step(steps - 1)
-            ke = s.stats()["ke_sum"] / N
+            curve = []
+            done = 0
+            while done < steps:
+                k = min(every, steps - done)
+                s.step(k)
+                done += k
+                curve.append(s.stats()["ke_sum"] / N)
+            s.synchronize()
+            fields = [_device_field(p_, N, torch) for p_ in s.macro_ptrs()]
+            b = ncomp * esz * 2
+            res = {"mlups": round(mlups, 1), "us_per_step": round(ms * 1e3 / args.steps, 1),
+                   "roofline_frac": round(N * b / (ms * 1e-3 / args.steps) / 1e9 / peak, 4), "bytes_per_cell": b,
+                   "us_launch_a_b": [round(statistics.median(t[0::2]), 1), round(statistics.median(t[1::2]), 1)],
+                   "ke_final_over_initial": curve[-1] / (curve[0] if curve else 1.0)}
+            if sto == STORE_F64:
+                ref_curve = np.array(curve)
+                ref_ke_end[mname] = curve[-1]
+                ref_fields[mname] = [f.clone() for f in fields]
+            else:
+                c = np.array(curve)
+                res["ke_max_rel_err_vs_f64"] = float(np.max(np.abs(c - ref_curve) / ref_curve))
+                rf = ref_fields[mname]
+                res["rho_minus_1_rel_l2_vs_f64"] = _rel_l2(fields[0] - 1.0, rf[0] - 1.0)
+                res["u_rel_l2_vs_f64"] = _rel_l2(torch.stack(fields[1:]), torch.stack(rf[1:]))
+            del fields
             s.close()
-            if sto == STORE_F32:
-                ref_ke = ke
-            b = bytes_cell[(mname, sto)]
-            out[f"{mname}_{sname}"] = {
-                "mlups": round(mlups, 1), "us_per_step": round(ms * 1e3 / args.steps, 1),
-                "roofline_frac": round(N * b / (ms * 1e-3 / args.steps) / 1e9 / peak, 4), "bytes_per_cell": b,
-                "us_launch_a_b": [round(statistics.median(split[0]), 1), round(statistics.median(split[1]), 1)],
-                "ke_decay": ke / ke0, "ke_rel_err_vs_f32": abs(ke - ref_ke) / ref_ke}
+            out[f"{mname}_{sname}"] = res
         for sname in ("f16", "bf16"):
             out[f"{mname}_{sname}"]["speedup_vs_f32"] = round(
                 out[f"{mname}_{sname}"]["mlups"] / out[f"{mname}_f32"]["mlups"], 3)
+    # the reference's own HOME on the same case (FP32): time and error against FP64
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_bind import RefCUDA
+    if RefCUDA.available():
+        R = RefCUDA()
+        h = R.create(1, (n, n, n), 0.51)
+        try:
+            host = [x.cpu().numpy() for x in (rho, u, v, w)]
+            R.set_mask(h, np.zeros((n, n, n), np.uint8))
+            R.init_fields(h, *host)
+            ms = R.time_steps(h, args.steps, 1)
+            R.init_fields(h, *host)
+            R.time_steps(h, steps, 1)
+            rr, ru, rv, rw = [torch.from_numpy(a.ravel()).cuda() for a in R.macros(h, (n, n, n))]
+            rf = ref_fields["home"]
+            ke = 0.5 * float((ru.double() ** 2 + rv.double() ** 2 + rw.double() ** 2).sum().item()) / N
+            out["home_reference_build"] = {
+                "mlups": round(N * args.steps / (ms * 1e-3) / 1e6, 1), "us_per_step": round(ms * 1e3 / args.steps, 1),
+                "call": "LBM3D_Home::step(1) per step (synchronous)",
+                "ke_rel_err_vs_f64_at_end": abs(ke - ref_ke_end["home"]) / ref_ke_end["home"],
+                "rho_minus_1_rel_l2_vs_f64": _rel_l2(rr - 1.0, rf[0] - 1.0),
+                "u_rel_l2_vs_f64": _rel_l2(torch.stack([ru, rv, rw]), torch.stack(rf[1:]))}
+        finally:
+            R.destroy(h)
+    out["legacy_reference_build"] = {"unavailable": "the reference's Legacy step indexes populations with int32 "
+                                                    "(src/lbm/lbm3d_legacy.cu:73,94-106): 19 x 512^3 overflows"}
     print(json.dumps({"study": "precision", "workload": f"TGV {n}^3 periodic, tau 0.51, u0 0.05, "
-                      f"{args.steps} timed steps, KE after {steps} steps", "results": out}))
+                      f"{args.steps} timed steps; KE every {every} steps up to {steps}, fields at {steps}",
+                      "hbm_peak_gbs": {"value": peak, "source": peak_kind}, "results": out}))
 
 
 def batch_instances(count=64, seed=20261203):
@@ -812,16 +961,45 @@ def slab_study(args, torch):
     print(json.dumps(out))
 
 
+def profile_tgv(args, torch):
+    """Set-up of the periodic Taylor-Green vortex of --profile-n^3 cells (tau 0.51,
+    u0 0.05; the precision study's field), --profile-method in --profile-storage,
+    macro output off, then 6 single steps: the case the narrow-storage ncu
+    captures run (`-k regex:aa_odd -s 1 -c 1` takes the second odd step)."""
+    from myfluidsimulation_b200.solvers import METHOD_HOME, METHOD_LEGACY, STORE_BF16, STORE_F16, STORE_F32, Solver
+    n = args.profile_n
+    rho, u, v, w = tgv_fields(n, torch)
+    sto = {"f32": STORE_F32, "f16": STORE_F16, "bf16": STORE_BF16}[args.profile_storage]
+    m = METHOD_HOME if args.profile_method == "home" else METHOD_LEGACY
+    st = torch.cuda.current_stream()
+    s = Solver(n, n, n, 0.51, method=m, storage=sto, stream=st.cuda_stream)
+    s.reinit_from_macro(rho, u, v, w)
+    s.set_macro_output(False)
+    for _ in range(6):
+        s.step(1)
+    s.synchronize()
+    s.close()
+    print(json.dumps({"profile": "tgv", "n": n, "method": args.profile_method, "storage": args.profile_storage,
+                      "steps": 6}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--methods", default="legacy,home,hybrid")
+    ap.add_argument("--methods", default=",".join(run_key(m, w) for m, w in RUNS),
+                    help="comma list of run keys: legacy, home, hybrid (periodic workload), *_inlet (inlet duct); "
+                         "the first is the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", default=None,
-                    help="set up METHOD on the workload and run 4 LBM steps only (for ncu captures)")
+                    help="set up one run key (e.g. legacy, home_inlet) on the duct, or 'tgv' (the periodic "
+                         "Taylor-Green vortex of --profile-n^3 cells, Legacy, --profile-storage), and run 4 LBM "
+                         "steps only (for ncu captures)")
+    ap.add_argument("--profile-n", type=int, default=256)
+    ap.add_argument("--profile-storage", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--profile-method", default="legacy", choices=["legacy", "home"])
     ap.add_argument("--study", default=None, choices=["precision", "batch", "adjoint", "vtk", "render", "slab"],
                     help="precision: 512^3 TGV MLUPS and kinetic-energy error of F32/F16/BF16 storage; "
                          "batch: 64 uneven Hybrid(B0) ducts in one persistent launch per step; "
@@ -836,6 +1014,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=2000)
     ap.add_argument("--tgv-n", type=int, default=512)
     ap.add_argument("--tgv-steps", type=int, default=2000)
+    ap.add_argument("--tgv-every", type=int, default=100)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -859,29 +1038,21 @@ def main():
 
     import myfluidsimulation_b200 as P
     P.lib()
-    if args.study == "precision":
-        precision_study(args, torch)
+    studies = {"precision": precision_study, "batch": batch_study, "adjoint": adjoint_study, "vtk": vtk_study,
+               "render": render_study, "slab": slab_study}
+    if args.study:
+        studies[args.study](args, torch)
         return
-    if args.study == "batch":
-        batch_study(args, torch)
-        return
-    if args.study == "adjoint":
-        adjoint_study(args, torch)
-        return
-    if args.study == "vtk":
-        vtk_study(args, torch)
-        return
-    if args.study == "render":
-        render_study(args, torch)
-        return
-    if args.study == "slab":
-        slab_study(args, torch)
+    if args.profile == "tgv":
+        profile_tgv(args, torch)
         return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)
+    keys = {run_key(m, w): (m, w) for m, w in RUNS}
     if args.profile:
         st = torch.cuda.current_stream()
-        s, _ = make_solver(args.profile, mask, st.cuda_stream)
+        m, w = keys[args.profile]
+        s, _ = make_solver(m, w, mask, st.cuda_stream)
         s.enable_stats(False)
         for _ in range(4):
             s.step(1)
@@ -889,18 +1060,21 @@ def main():
         s.close()
         print(json.dumps({"profile": args.profile, "steps": 4}))
         return
-    methods = [m for m in args.methods.split(",") if m]
+    runs = [k for k in args.methods.split(",") if k]
+    for k in runs:
+        if k not in keys:
+            raise SystemExit(f"unknown run key {k!r}; known: {', '.join(keys)}")
     peak, peak_kind = measured_peaks()
     N = NX * NY * NZ
     results = {}
-    clocks = None
-    head = methods[0]
-    clk = ClockSampler(local).__enter__()   # spans the timed regions of all methods
-    for mth in methods:
+    head = runs[0]
+    clk = ClockSampler(local).__enter__()   # spans the timed regions of all runs
+    for key in runs:
+        mth, wl = keys[key]
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        s, r = run_method(mth, mask, args, torch, rank)
+        s, r = run_method(mth, wl, mask, args, torch)
         ms = torch.tensor([r["ms_total"]], device="cuda")
         if dist:
             dist.all_reduce(ms, op=dist.ReduceOp.MAX)
@@ -910,25 +1084,30 @@ def main():
         per_launch_ms = r["ms_total"] / (DRAG_EVERY * args.steps)
         achieved = N * BYTES[mth] / (per_launch_ms * 1e-3) / 1e9
         tr = profile_traffic(mth)
-        results[mth] = {"mlups": round(mlups, 1), "ms_per_step": round(ms / args.steps, 4),
-                        "kernel_us": r["kernel_us"],
+        ku = r["kernel_us"]
+        split_ms = DRAG_EVERY * sum(ku.values()) / len(ku) / 1e3
+        results[key] = {"mlups": round(mlups, 1), "ms_per_step": round(ms / args.steps, 4),
+                        "workload": wl, "kernel_us": ku,
+                        "kernel_split_ms_per_step": round(split_ms, 4),
                         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                                      "frac": round(achieved / peak, 4),
                                      "traffic": None if tr is None else int(round(tr * N)),
                                      "kernel": KERNEL[mth], "bytes_per_cell": BYTES[mth]},
+                        "kernel_frac": {k: round(N * BYTES[mth] / (v * 1e-6) / 1e9 / peak, 4) for k, v in ku.items()},
                         "drag": [round(x, 6) for x in r["drag_last"]], "mass": round(r["mass"], 3),
                         "launches": r["launches"]}
         if mth == "hybrid":
-            results[mth]["band_cells"] = r["band_cells"]
-        if mth == head:
+            results[key]["band_cells"] = r["band_cells"]
+        if key == head:
             head_solver = s
         else:
             s.close()
 
     clk.__exit__()
     clocks = clk.summary()
-    # end to end through the C-ABI with host buffers (headline method)
-    e2e_ms, e2e_wall, h2d, d2h = e2e_run(head, mask, args, torch)
+    # end to end through the C-ABI with host buffers (headline run)
+    hm, hw = keys[head]
+    e2e_ms, e2e_wall, h2d, d2h = e2e_run(hm, hw, mask, args, torch)
     e2e_t = torch.tensor([e2e_ms], device="cuda")
     if dist:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
@@ -936,10 +1115,10 @@ def main():
 
     cpu = None
     l2 = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and head == "legacy":
         def gpu_state(steps):
             st = torch.cuda.current_stream()
-            g, _ = make_solver(head, mask, st.cuda_stream)
+            g, _ = make_solver("legacy", "periodic", mask, st.cuda_stream)
             g.enable_stats(False)
             g.step(steps)
             g.synchronize()
@@ -954,16 +1133,16 @@ def main():
 
     if rank == 0:
         h = results[head]
+        config = dict(HEAD_CONFIG) if head == "legacy" else {
+            "workload": WORKLOAD_TEXT[hw], "method": hm, "storage": "f32", "l2": HEAD_CONFIG["l2"]}
+        if world > 1:
+            config["parallelism"] = f"replicas x{world}"
         line = {
-            "metric": "D3Q19 MLUPS (Legacy BGK FP32, duct 256x128x128 past a voxelized sphere)",
+            "metric": METRIC,
             "value": h["mlups"], "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": h["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "duct 256x128x128, inlet u=0.05, outflow, y/z walls, icosphere "
-                                   f"({ntri} triangles, r=16, {nsph} solid cells) voxelized on the GPU, tau 0.56; "
-                                   "one step = 50 LBM steps + drag",
-                       "method": head, "storage": "f32", "bounce": "halfway (AA in-place)",
-                       "l2": "inputs larger than L2 (319 MB FP32 state)", "parallelism": f"replicas x{world}"},
+            "dtype": "f32", "data": "synthetic", "config": config,
+            "bounce": "halfway bounce-back, AA pattern in place",
             "roofline": dict(h["roofline"], peak_kind=peak_kind),
             "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "wall_ms": round(e2e_wall, 2)},
@@ -974,8 +1153,8 @@ def main():
         if cpu is not None:
             line["cpu_baseline"] = cpu
         if l2 is not None:
-            line["l2_vs_fp64"] = {"value": l2, "what": f"relative L2 of the {head} state vs the FP64 oracle",
-                                  "steps": l2_steps}
+            line["l2_vs_fp64"] = {"value": l2, "what": "relative L2 of the Legacy state vs the FP64 oracle "
+                                                       "(periodic workload)", "steps": l2_steps}
         print(json.dumps(line))
     if dist:
         dist.barrier()

@@ -41,8 +41,11 @@ enum {
 
 /* collision / update method (the reference's three solver classes) */
 enum { LBM_METHOD_LEGACY = 0, LBM_METHOD_HOME = 1, LBM_METHOD_HYBRID = 2 };
-/* storage of populations (Legacy/Hybrid) or moments (HOME) */
-enum { LBM_STORE_F32 = 0, LBM_STORE_F16 = 1, LBM_STORE_BF16 = 2 };
+/* storage of populations (Legacy/Hybrid) or moments (HOME).
+ * F16/BF16 keep shifted values (f - w_q rho0; HOME: rho - rho0, u, S) and
+ * compute in FP32.  F64 stores and computes in FP64: the reference form the
+ * others are measured against (Legacy/Hybrid with halfway bounce-back; HOME). */
+enum { LBM_STORE_F32 = 0, LBM_STORE_F16 = 1, LBM_STORE_BF16 = 2, LBM_STORE_F64 = 3 };
 /* boundary: fully periodic (the reference), or a duct along x with a
  * velocity inlet at x=0 and a zero-gradient outlet at x=Nx-1 */
 enum { LBM_BC_PERIODIC = 0, LBM_BC_DUCT = 1 };
@@ -397,8 +400,8 @@ int lbm_set_z_ghosts(lbm_solver* s, int on);
  * buffer (they move to the other buffer with every step), each *bytes long. */
 int lbm_zslab_moment_planes(lbm_solver* s, int plane, void** ptrs, int64_t* bytes);
 /* Index of this solver's cell 0 in the whole grid (a slab: its plane 0).  Only
- * HOME's F16/BF16 stochastic rounding reads it, so that a slab draws the same
- * random bits for a cell as the whole grid does. */
+ * the F16/BF16 stochastic rounding (every method) reads it, so that a slab
+ * draws the same random bits for a cell as the whole grid does. */
 int lbm_set_index_base(lbm_solver* s, int64_t base);
 /* Device addresses of the 5 slot planes of `plane` whose direction has
  * c_z = cz (+1 or -1), in direction order, each *bytes long: what crosses a

@@ -18,7 +18,7 @@ ERRORS = {1: "LBM_ERR_INVALID", 2: "LBM_ERR_CUDA", 3: "LBM_ERR_ALLOC", 4: "LBM_E
           5: "LBM_ERR_IO", 6: "LBM_ERR_UNSUPPORTED", 7: "LBM_ERR_TIMEOUT"}
 
 METHOD_LEGACY, METHOD_HOME, METHOD_HYBRID = 0, 1, 2
-STORE_F32, STORE_F16, STORE_BF16 = 0, 1, 2
+STORE_F32, STORE_F16, STORE_BF16, STORE_F64 = 0, 1, 2, 3
 VTK_SCALAR, VTK_SPEED, VTK_VECTOR = 0, 1, 2
 FILTER_EXACT, FILTER_TEXTURE = 0, 1
 BC_PERIODIC, BC_DUCT = 0, 1

@@ -27,30 +27,37 @@
 namespace lbm {
 namespace {
 
-struct Cell {
-    float r, ux, uy, uz;
+template <class R>
+struct CellT {
+    R r, ux, uy, uz;
 };
+using Cell = CellT<float>;
+
+__device__ __forceinline__ float rfma(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double rfma(double a, double b, double c) { return fma(a, b, c); }
 
 // Pre-collision moments with the velocity-shift force (legacy.cu:78-90).
 // Opposite pairs are summed first: s = f_q + f_opp, d = f_q - f_opp.
-__device__ __forceinline__ Cell moments(const float (&f)[19], float fx, float fy, float fz) {
+// R: float, or double for the FP64 reference form.
+template <class R>
+__device__ __forceinline__ CellT<R> moments(const R (&f)[19], R fx, R fy, R fz) {
     // pairs with their positive member: (1,2) x, (3,4) y, (5,6) z, (7,10) +x+y,
     // (9,8) +x-y, (11,14) +x+z, (13,12) +x-z, (15,18) +y+z, (17,16) +y-z
-    const float s12 = f[1] + f[2], d12 = f[1] - f[2];
-    const float s34 = f[3] + f[4], d34 = f[3] - f[4];
-    const float s56 = f[5] + f[6], d56 = f[5] - f[6];
-    const float s7 = f[7] + f[10], d7 = f[7] - f[10];
-    const float s9 = f[9] + f[8], d9 = f[9] - f[8];
-    const float s11 = f[11] + f[14], d11 = f[11] - f[14];
-    const float s13 = f[13] + f[12], d13 = f[13] - f[12];
-    const float s15 = f[15] + f[18], d15 = f[15] - f[18];
-    const float s17 = f[17] + f[16], d17 = f[17] - f[16];
-    Cell c;
+    const R s12 = f[1] + f[2], d12 = f[1] - f[2];
+    const R s34 = f[3] + f[4], d34 = f[3] - f[4];
+    const R s56 = f[5] + f[6], d56 = f[5] - f[6];
+    const R s7 = f[7] + f[10], d7 = f[7] - f[10];
+    const R s9 = f[9] + f[8], d9 = f[9] - f[8];
+    const R s11 = f[11] + f[14], d11 = f[11] - f[14];
+    const R s13 = f[13] + f[12], d13 = f[13] - f[12];
+    const R s15 = f[15] + f[18], d15 = f[15] - f[18];
+    const R s17 = f[17] + f[16], d17 = f[17] - f[16];
+    CellT<R> c;
     c.r = f[0] + ((s12 + s34) + (s56 + s7)) + ((s9 + s11) + (s13 + s15) + s17);
-    const float jx = (d12 + d7) + (d9 + d11) + d13;
-    const float jy = (d34 + d7) - d9 + (d15 + d17);
-    const float jz = (d56 + d11) - d13 + (d15 - d17);
-    const float inv = c.r > 0.f ? 1.0f / c.r : 0.f;
+    const R jx = (d12 + d7) + (d9 + d11) + d13;
+    const R jy = (d34 + d7) - d9 + (d15 + d17);
+    const R jz = (d56 + d11) - d13 + (d15 - d17);
+    const R inv = c.r > R(0) ? R(1) / c.r : R(0);
     c.ux = jx * inv + fx;
     c.uy = jy * inv + fy;
     c.uz = jz * inv + fz;
@@ -60,17 +67,18 @@ __device__ __forceinline__ Cell moments(const float (&f)[19], float fx, float fy
 // BGK collision f* = f + w (feq - f) for every direction, the equilibrium
 // evaluated per opposite pair: feq_(+-) = w rho (1 - 1.5u^2 + 4.5 t^2) +- 3 w rho t.
 // (The Hybrid's "HOME form" of hybrid.cu:148-152 is this with w = omega_shear.)
-__device__ __forceinline__ void collide(float (&f)[19], const Cell& c, float omega) {
-    const float A = 1.0f - 1.5f * (c.ux * c.ux + c.uy * c.uy + c.uz * c.uz);
+template <class R>
+__device__ __forceinline__ void collide(R (&f)[19], const CellT<R>& c, R omega) {
+    const R A = R(1) - R(1.5) * (c.ux * c.ux + c.uy * c.uy + c.uz * c.uz);
     // w_q rho with the weights' own rounding compensated (mulk): no mass or momentum bias per step
-    const float r0 = mulk(c.r, K3_HI, K3_LO), r1 = mulk(c.r, K18_HI, K18_LO), r2 = mulk(c.r, K36_HI, K36_LO);
-    auto pair = [&](int qp, int qm, float t, float wr) {
-        const float sym = wr * fmaf(4.5f * t, t, A);
-        const float asym = 3.0f * wr * t;
-        f[qp] = fmaf(omega, (sym + asym) - f[qp], f[qp]);
-        f[qm] = fmaf(omega, (sym - asym) - f[qm], f[qm]);
+    const R r0 = mulk(c.r, K3_HI, K3_LO), r1 = mulk(c.r, K18_HI, K18_LO), r2 = mulk(c.r, K36_HI, K36_LO);
+    auto pair = [&](int qp, int qm, R t, R wr) {
+        const R sym = wr * rfma(R(4.5) * t, t, A);
+        const R asym = R(3) * wr * t;
+        f[qp] = rfma(omega, (sym + asym) - f[qp], f[qp]);
+        f[qm] = rfma(omega, (sym - asym) - f[qm], f[qm]);
     };
-    f[0] = fmaf(omega, r0 * A - f[0], f[0]);
+    f[0] = rfma(omega, r0 * A - f[0], f[0]);
     pair(1, 2, c.ux, r1);
     pair(3, 4, c.uy, r1);
     pair(5, 6, c.uz, r1);
@@ -137,7 +145,8 @@ __device__ __forceinline__ void collide_g(float (&g)[19], const Cell& c, float d
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
 // Momentum exchanged with obstacle cells along the solid links of one cell.
-__device__ __noinline__ void add_drag(double* acc, const float* o, uint32_t lk, const uint8_t* flags, int x, int y,
+template <class R>
+__device__ __noinline__ void add_drag(double* acc, const R* o, uint32_t lk, const uint8_t* flags, int x, int y,
                                       int z, int nx, int ny, int nz, int duct) {
     for (int q = 1; q < 19; ++q) {
         if (!((lk >> q) & 1u)) continue;
@@ -161,7 +170,8 @@ __device__ __noinline__ void add_drag_g(double* acc, const float* o, float invS,
     add_drag(acc, f, lk, flags, x, y, z, nx, ny, nz, duct);
 }
 
-__device__ __forceinline__ void add_cell_stats(double (&acc)[NSTAT], const Cell& c) {
+template <class R>
+__device__ __forceinline__ void add_cell_stats(double (&acc)[NSTAT], const CellT<R>& c) {
     acc[0] += (double)c.r;
     acc[1] += 0.5 * ((double)c.ux * c.ux + (double)c.uy * c.uy + (double)c.uz * c.uz);
     acc[5] += (double)c.r * c.ux;
@@ -173,6 +183,9 @@ __device__ __forceinline__ void add_cell_stats(double (&acc)[NSTAT], const Cell&
 // (rho, (u_in,0,0)) of a direction with c_x = +1 is w rho (1 + 3u + 3u^2);
 // `kin` = 1 + 3u + 3u^2.
 __device__ __forceinline__ float inlet_value(int q, float r, float kin) { return wq(q) * r * kin; }
+__device__ __forceinline__ double inlet_value(int q, double r, double kin) {
+    return (q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0)) * r * kin;
+}
 // the same in stored units: S w (rho kin - rho0)
 __device__ __forceinline__ float inlet_g(int q, float r, float kin, float r0, float S) {
     return S * (wq(q) * fmaf(r, kin, -r0));
@@ -187,18 +200,22 @@ template <class ST, bool MASK, int VEC, int MODE, class IDX>
 __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc)[NSTAT]) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     using T = typename ST::T;
+    using R = typename Real<ST>::type;
     T* __restrict__ f = static_cast<T*>(p.f);
     const IDX N = (IDX)p.N;
-    const float kin = 1.0f + 3.0f * p.u_in + 3.0f * p.u_in * p.u_in;
+    const R kin = R(1) + R(3) * p.u_in + R(3) * p.u_in * p.u_in;
     {
-        constexpr bool SH = ST::kId != 0;   // narrow forms: compute in stored units
+        constexpr bool SH = kNarrow<ST>;    // narrow forms: compute in stored units
         const IDX id = v * VEC;
-        float a[19][VEC];
+        R a[19][VEC];
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             if constexpr (SH) ldv_raw<ST, VEC>(f + (IDX)q * N + id, a[q]);
             else ldv<ST, VEC>(f + (IDX)q * N + id, q, p.rho0, a[q]);
         }
+        // narrow forms: stochastically rounded stores, random words from one
+        // hash of the first cell's global index and its loaded rest population
+        const uint32_t hsr = SH ? sr_seed((uint32_t)id + p.salt_base, (float)a[0][0]) : 0u;
         uint32_t fl4 = 0;
         if constexpr (MASK) {
             if constexpr (VEC == 4) fl4 = *reinterpret_cast<const uint32_t*>(p.flags + id);
@@ -211,18 +228,20 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
 #pragma unroll
         for (int l = 0; l < VEC; ++l) {
             const uint32_t fl = (fl4 >> (8 * l)) & 0xffu;
-            float c[19];
+            R c[19];
 #pragma unroll
             for (int q = 0; q < 19; ++q) c[q] = a[q][l];
-            float dr = 0.f;
-            const Cell m = SH ? moments_g(c, p.fx, p.fy, p.fz, p.rho0, Raw<ST>::invS, dr) : moments(c, p.fx, p.fy, p.fz);
+            R dr = 0;
+            CellT<R> m;
+            if constexpr (SH) m = moments_g(c, p.fx, p.fy, p.fz, p.rho0, Raw<ST>::invS, dr);
+            else m = moments<R>(c, p.fx, p.fy, p.fz);
             const bool solid = MASK && (fl & F_SOLID);
             const float om = (p.hybrid && !(fl & F_BAND)) ? p.omega_s : p.omega;
-            float o[19];
+            R o[19];
 #pragma unroll
             for (int q = 0; q < 19; ++q) o[q] = c[q];
             if constexpr (SH) collide_g(o, m, dr, om, Raw<ST>::S);
-            else collide(o, m, om);
+            else collide<R>(o, m, R(om));
             if (STATS && !solid) {
                 add_cell_stats(acc, m);
                 if (MASK && (fl & F_TOUCH)) {
@@ -241,20 +260,24 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
             const bool at_in = p.duct && x == 0, at_out = p.duct && x == p.nx - 1;
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
-                float v = o[q];
-                if (cx(q) < 0) v = at_in ? (SH ? inlet_g(q, m.r, kin, p.rho0, Raw<ST>::S) : inlet_value(q, m.r, kin)) : v;
+                R v = o[q];
+                if constexpr (SH) {
+                    if (cx(q) < 0) v = at_in ? inlet_g(q, m.r, kin, p.rho0, Raw<ST>::S) : v;
+                } else {
+                    if (cx(q) < 0) v = at_in ? inlet_value(q, m.r, kin) : v;
+                }
                 if (cx(q) > 0) v = at_out ? o[opp(q)] : v;
                 // a solid cell keeps its populations (legacy.cu:72-76): slot opp(q) gets its own value
                 a[q][l] = solid ? c[opp(q)] : v;
             }
-            mr[l] = solid ? 1.f : m.r;
-            mu[l] = solid ? 0.f : m.ux;
-            mv[l] = solid ? 0.f : m.uy;
-            mw[l] = solid ? 0.f : m.uz;
+            mr[l] = solid ? 1.f : (float)m.r;
+            mu[l] = solid ? 0.f : (float)m.ux;
+            mv[l] = solid ? 0.f : (float)m.uy;
+            mw[l] = solid ? 0.f : (float)m.uz;
         }
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
-            if constexpr (SH) stv_raw<ST, VEC>(f + (IDX)opp(q) * N + id, a[q]);
+            if constexpr (SH) stv_raw_sr<ST, VEC>(f + (IDX)opp(q) * N + id, a[q], hsr, q);
             else stv<ST, VEC>(f + (IDX)opp(q) * N + id, q, p.rho0, a[q]);
         }
         if constexpr (MACRO) {
@@ -308,12 +331,13 @@ struct Nbr {
 template <class ST, bool MASK, int MODE, class IDX>
 __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, double (&acc)[NSTAT]) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
-    constexpr bool SH = ST::kId != 0;   // narrow forms: compute in stored units
+    constexpr bool SH = kNarrow<ST>;    // narrow forms: compute in stored units
     using T = typename ST::T;
+    using R = typename Real<ST>::type;
     T* __restrict__ f = static_cast<T*>(p.f);
     const IDX N = (IDX)p.N;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
-    const float kin = 1.0f + 3.0f * p.u_in + 3.0f * p.u_in * p.u_in;
+    const R kin = R(1) + R(3) * p.u_in + R(3) * p.u_in * p.u_in;
     {
         const int y = (int)(row % ny);
         const int z = (int)(row / ny);
@@ -327,7 +351,7 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, doub
         nb.init(x, y, z, nx, ny, nz);
         uint32_t lk = 0u;
         if (MASK && (fl & F_SPECIAL)) lk = p.links[id];
-        float c[19];
+        R c[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             // incoming q travels the link x -> x + c_opp(q); if that link does not
@@ -337,27 +361,33 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, doub
             if constexpr (SH) c[q] = Raw<ST>::ld(f + src);
             else c[q] = ST::ld(f + src, q, p.rho0);
         }
-        float dr = 0.f;
-        const Cell m = SH ? moments_g(c, p.fx, p.fy, p.fz, p.rho0, Raw<ST>::invS, dr) : moments(c, p.fx, p.fy, p.fz);
+        R dr = 0;
+        CellT<R> m;
+        if constexpr (SH) m = moments_g(c, p.fx, p.fy, p.fz, p.rho0, Raw<ST>::invS, dr);
+        else m = moments<R>(c, p.fx, p.fy, p.fz);
+        const uint32_t hsr = SH ? sr_seed((uint32_t)id + p.salt_base, (float)c[0]) : 0u;   // stochastic rounding
         const float om = (p.hybrid && !(fl & F_BAND)) ? p.omega_s : p.omega;
-        float o[19];
+        R o[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) o[q] = c[q];
         if constexpr (SH) collide_g(o, m, dr, om, Raw<ST>::S);
-        else collide(o, m, om);
+        else collide<R>(o, m, R(om));
         const bool at_in = p.duct && x == 0, at_out = p.duct && x == nx - 1;
 #pragma unroll
         for (int q = 0; q < 19; ++q) {
             const bool nn = (lk >> q) & 1u;
-            float v = o[q];
-            if (cx(q) < 0)
-                v = (nn && at_in) ? (SH ? inlet_g(q, m.r, kin, p.rho0, Raw<ST>::S) : inlet_value(q, m.r, kin)) : v;
+            R v = o[q];
+            if constexpr (SH) {
+                if (cx(q) < 0) v = (nn && at_in) ? inlet_g(q, m.r, kin, p.rho0, Raw<ST>::S) : v;
+            } else {
+                if (cx(q) < 0) v = (nn && at_in) ? inlet_value(q, m.r, kin) : v;
+            }
             if (cx(q) > 0) v = (nn && at_out) ? o[opp(q)] : v;
             const IDX dst = nn ? ((IDX)opp(q) * N + id) : ((IDX)q * N + nb.at(cx(q), cy(q), cz(q)));
-            if constexpr (SH) Raw<ST>::st(f + dst, v);
+            if constexpr (SH) Raw<ST>::st_sr(f + dst, v, sr_word(hsr, 2 * q));
             else ST::st(f + dst, q, p.rho0, v);
         }
-        if (MACRO) { p.rho[id] = m.r; p.ux[id] = m.ux; p.uy[id] = m.uy; p.uz[id] = m.uz; }
+        if (MACRO) { p.rho[id] = (float)m.r; p.ux[id] = (float)m.ux; p.uy[id] = (float)m.uy; p.uz[id] = (float)m.uz; }
         if (STATS) {
             add_cell_stats(acc, m);
             if (MASK && (fl & F_TOUCH)) {
@@ -370,7 +400,7 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, doub
 
 // Odd step: one cell per thread, rows of blockDim.x cells per block iteration.
 template <class ST, bool MASK, int MODE, class IDX>
-__global__ void __launch_bounds__(256, MASK ? 4 : 3) aa_odd(AAParams p) {
+__global__ void __launch_bounds__(256, ST::kId == 3 ? 2 : (MASK ? 4 : 3)) aa_odd(AAParams p) {
     constexpr bool STATS = MODE == 2;
     const int bx = blockDim.x;
     const int segs = (p.nx + bx - 1) / bx;
@@ -418,8 +448,9 @@ __global__ void aa_materialize(AAParams p, int parity, float* __restrict__ out) 
 template <class ST, int MODE, class IDX>
 void launch_mode(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
     const bool mask = p.flags != nullptr;
-    // consecutive cells per thread: two in FP32 (8-byte accesses), four in F16/BF16 (8-byte accesses)
-    constexpr int V = ST::kId == 0 ? 2 : 4;
+    // consecutive cells per thread: two in FP32 (8-byte accesses), four in F16/BF16 (8-byte
+    // accesses), one in FP64 (8-byte accesses)
+    constexpr int V = ST::kId == 0 ? 2 : (ST::kId == 3 ? 1 : 4);
     if (parity == 0) {
         const int64_t span = p.first | p.cells;      // both must be multiples of the vector width
         if (V == 4 && span % 4 != 0 && span % 2 == 0) {
@@ -568,6 +599,7 @@ cudaError_t launch_aa_step(const AAParams& p, int storage, int parity, LaunchCfg
         case 0: return launch_typed<StoreF32>(p, parity, cfg, s);
         case 1: return launch_typed<StoreF16>(p, parity, cfg, s);
         case 2: return launch_typed<StoreBF16>(p, parity, cfg, s);
+        case 3: return launch_typed<StoreF64>(p, parity, cfg, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -578,6 +610,7 @@ cudaError_t launch_aa_materialize(const AAParams& p, int storage, int parity, fl
         case 0: aa_materialize<StoreF32><<<blocks, 256, 0, s>>>(p, parity, out); break;
         case 1: aa_materialize<StoreF16><<<blocks, 256, 0, s>>>(p, parity, out); break;
         case 2: aa_materialize<StoreBF16><<<blocks, 256, 0, s>>>(p, parity, out); break;
+        case 3: aa_materialize<StoreF64><<<blocks, 256, 0, s>>>(p, parity, out); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -46,6 +46,25 @@ __global__ void aa_reinit(typename ST::T* f, float r0, int64_t N, const float* r
     }
 }
 
+// FP64 storage: the equilibrium of the (FP32) macro fields evaluated in FP64
+__global__ void aa_reinit_f64(double* f, int64_t N, const float* rho, const float* ux, const float* uy,
+                              const float* uz, float* ro, float* uo, float* vo, float* wo) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const double r = rho ? rho[i] : 1.0;
+        const double u = ux ? ux[i] : 0.0;
+        const double v = uy ? uy[i] : 0.0;
+        const double w = uz ? uz[i] : 0.0;
+        const double uu = u * u + v * v + w * w;
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const double cu = (double)cx(q) * u + (double)cy(q) * v + (double)cz(q) * w;
+            const double wd = q == 0 ? 1.0 / 3.0 : (q <= 6 ? 1.0 / 18.0 : 1.0 / 36.0);
+            f[q * N + i] = wd * r * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * uu);
+        }
+        if (ro) { ro[i] = (float)r; uo[i] = (float)u; vo[i] = (float)v; wo[i] = (float)w; }
+    }
+}
+
 template <class T> __device__ __forceinline__ void st_mom(T* p, int k, float r0, float v);
 template <> __device__ __forceinline__ void st_mom<float>(float* p, int k, float r0, float v) { *p = v; }
 template <> __device__ __forceinline__ void st_mom<__half>(__half* p, int k, float r0, float v) {
@@ -54,6 +73,7 @@ template <> __device__ __forceinline__ void st_mom<__half>(__half* p, int k, flo
 template <> __device__ __forceinline__ void st_mom<__nv_bfloat16>(__nv_bfloat16* p, int k, float r0, float v) {
     *p = __float2bfloat16_rn(k == 0 ? v - r0 : v);
 }
+template <> __device__ __forceinline__ void st_mom<double>(double* p, int k, float r0, float v) { *p = v; }
 
 // src/lbm/lbm3d_home.cu:109-137 (m = mnext = (rho, u, S = 0))
 template <class T>
@@ -228,6 +248,7 @@ cudaError_t launch_aa_reinit(void* f, int storage, float rho0, int64_t N, const 
         case 0: aa_reinit<StoreF32><<<g, 256, 0, s>>>((float*)f, rho0, N, rho, ux, uy, uz, ro, uo, vo, wo, form); break;
         case 1: aa_reinit<StoreF16><<<g, 256, 0, s>>>((__half*)f, rho0, N, rho, ux, uy, uz, ro, uo, vo, wo, form); break;
         case 2: aa_reinit<StoreBF16><<<g, 256, 0, s>>>((__nv_bfloat16*)f, rho0, N, rho, ux, uy, uz, ro, uo, vo, wo, form); break;
+        case 3: aa_reinit_f64<<<g, 256, 0, s>>>((double*)f, N, rho, ux, uy, uz, ro, uo, vo, wo); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -240,6 +261,7 @@ cudaError_t launch_home_reinit(void* m, void* mn, int storage, float rho0, int64
         case 0: home_reinit<float><<<g, 256, 0, s>>>((float*)m, (float*)mn, rho0, N, rho, ux, uy, uz); break;
         case 1: home_reinit<__half><<<g, 256, 0, s>>>((__half*)m, (__half*)mn, rho0, N, rho, ux, uy, uz); break;
         case 2: home_reinit<__nv_bfloat16><<<g, 256, 0, s>>>((__nv_bfloat16*)m, (__nv_bfloat16*)mn, rho0, N, rho, ux, uy, uz); break;
+        case 3: home_reinit<double><<<g, 256, 0, s>>>((double*)m, (double*)mn, rho0, N, rho, ux, uy, uz); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

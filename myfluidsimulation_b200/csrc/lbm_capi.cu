@@ -65,7 +65,7 @@ struct lbm_solver {
     lbm::LaunchCfg cfg_even{0, 256}, cfg_odd{0, 256};
     int home_zchunk = 16;
     bool zghost = false;        // z-slab: planes 0 and nz-1 are ghosts, steps cover 1..nz-2
-    uint32_t salt_base = 0;     // HOME narrow stores: index of plane 0 in the whole grid
+    uint32_t salt_base = 0;     // narrow stores: index of cell 0 in the whole grid
     // graph cache
     cudaGraphExec_t gexec = nullptr;
     int g_sub = 0, g_parity = -1, g_stats = -1;
@@ -141,6 +141,7 @@ lbm::AAParams aa_params(lbm_solver* s, bool macro, bool stats) {
     const int64_t plane = (int64_t)s->dom.nx * s->dom.ny;
     p.first = s->zghost ? plane : 0;
     p.cells = s->zghost ? s->N - 2 * plane : s->N;
+    p.salt_base = s->salt_base;
     return p;
 }
 
@@ -269,6 +270,9 @@ static int merge_slots(lbm_solver* s, int plane, int cz, void* const* src, cudaS
         if (s->esize == 4)
             zslab_merge<uint32_t><<<blocks, 256, 0, st>>>(static_cast<uint32_t*>(dst[k]),
                                                           static_cast<const uint32_t*>(src[k]), fl, lk, pl, lbm::opp(q));
+        else if (s->esize == 8)
+            zslab_merge<uint64_t><<<blocks, 256, 0, st>>>(static_cast<uint64_t*>(dst[k]),
+                                                          static_cast<const uint64_t*>(src[k]), fl, lk, pl, lbm::opp(q));
         else
             zslab_merge<uint16_t><<<blocks, 256, 0, st>>>(static_cast<uint16_t*>(dst[k]),
                                                           static_cast<const uint16_t*>(src[k]), fl, lk, pl, lbm::opp(q));
@@ -292,7 +296,11 @@ int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out)
     o.rho0 = 1.0f;
     if (opts) o = *opts;
     if (o.method < 0 || o.method > 2) { set_error("lbm_create: bad method"); return LBM_ERR_INVALID; }
-    if (o.storage < 0 || o.storage > 2) { set_error("lbm_create: bad storage"); return LBM_ERR_INVALID; }
+    if (o.storage < 0 || o.storage > 3) { set_error("lbm_create: bad storage"); return LBM_ERR_INVALID; }
+    if (o.storage == LBM_STORE_F64 && o.method != LBM_METHOD_HOME && o.bounce == LBM_BOUNCE_REFERENCE) {
+        set_error("lbm_create: FP64 storage runs Legacy/Hybrid with halfway bounce-back only");
+        return LBM_ERR_UNSUPPORTED;
+    }
     if (o.bc < 0 || o.bc > 1) { set_error("lbm_create: bad boundary"); return LBM_ERR_INVALID; }
     if (o.bc == LBM_BC_DUCT && dom->nx < 3) { set_error("lbm_create: a duct needs nx >= 3"); return LBM_ERR_INVALID; }
     if (o.bounce < 0 || o.bounce > 1) { set_error("lbm_create: bad bounce mode"); return LBM_ERR_INVALID; }
@@ -315,7 +323,7 @@ int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out)
     s->omega = 1.0f / dom->tau;
     s->omega_s = s->omega;
     s->N = N;
-    s->esize = o.storage == LBM_STORE_F32 ? 4 : 2;
+    s->esize = o.storage == LBM_STORE_F32 ? 4 : (o.storage == LBM_STORE_F64 ? 8 : 2);
     auto fail = [&](int code) { lbm_destroy(s); return code; };
     if (o.stream) s->stream = static_cast<cudaStream_t>(o.stream);
     else {
@@ -332,12 +340,13 @@ int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out)
     s->cfg_even = {sms * 8, 256};
     s->cfg_odd = {sms * 12, 256};
     // HOME: the longest z-chunk (fewest re-built halo planes) that still gives
-    // three waves of blocks at 3 blocks per SM, so the tail of the last wave
-    // stays short (measured on B200: 256x128x128 best at 12, 512^3 at 48)
-    {
+    // three waves of resident blocks, so the tail of the last wave stays short
+    if (o.method == LBM_METHOD_HOME) {
+        static const int bps = lbm::home_blocks_per_sm();
         int zc = 4;
         for (int c : {48, 32, 24, 16, 12, 10, 8, 6, 4}) {
-            if ((int64_t)lbm::home_num_blocks(dom->nx, dom->ny, dom->nz, std::min(c, dom->nz)) >= (int64_t)sms * 9) {
+            if ((int64_t)lbm::home_num_blocks(dom->nx, dom->ny, dom->nz, std::min(c, dom->nz)) >=
+                (int64_t)sms * bps * 3) {
                 zc = c;
                 break;
             }
@@ -609,6 +618,16 @@ int lbm_step(lbm_solver* s, int substeps) {
 int lbm_step_graph(lbm_solver* s, int substeps) {
     if (!s) { set_error("lbm_step_graph: null solver"); return LBM_ERR_INVALID; }
     if (substeps <= 0) return lbm_step(s, substeps);
+    // A read-back queued on the copy stream (lbm_read_macros_async,
+    // lbm_get_stats_async) must end before the replayed steps rewrite the macro
+    // fields, the statistics or HOME's moment buffers.  The wait goes on the
+    // solver's stream before every launch, outside the graph: the read's event
+    // was recorded outside any capture, so it cannot be waited on inside one.
+    // Once waited for, read_pending is clear, so a capture below queues no wait.
+    {
+        const int rc = wait_pending_read(s);
+        if (rc != LBM_OK) return rc;
+    }
     const int par = is_aa(s) ? s->parity : s->cur;
     if (!s->gexec || s->g_sub != substeps || s->g_parity != par || s->g_stats != (int)s->stats_on) {
         drop_graph(s);
@@ -863,6 +882,7 @@ int lbm_zslab_plan_exchange(lbm_zslab_plan* p, int phase, void* stream) {
     const dim3 grid((unsigned)std::min<int64_t>((p->elems + 255) / 256, 1024), (unsigned)p->njobs);
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (p->esize == 4) zslab_jobs<uint32_t><<<grid, 256, 0, st>>>(p->d_jobs[phase]);
+    else if (p->esize == 8) zslab_jobs<uint64_t><<<grid, 256, 0, st>>>(p->d_jobs[phase]);
     else zslab_jobs<uint16_t><<<grid, 256, 0, st>>>(p->d_jobs[phase]);
     CK(cudaGetLastError());
     return LBM_OK;

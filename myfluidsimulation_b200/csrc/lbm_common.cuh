@@ -58,6 +58,8 @@ constexpr float K6_HI = 0x1.555556p-3f, K6_LO = -0x1.555556p-28f;     // 1/6
 constexpr float K18_HI = 0x1.c71c72p-5f, K18_LO = -0x1.c71c72p-32f;   // 1/18
 constexpr float K36_HI = 0x1.c71c72p-6f, K36_LO = -0x1.c71c72p-33f;   // 1/36
 __device__ __forceinline__ float mulk(float x, float hi, float lo) { return __fmaf_rn(hi, x, __fmul_rn(lo, x)); }
+// FP64: the constant itself to 48 bits (hi + lo), one product
+__device__ __forceinline__ double mulk(double x, float hi, float lo) { return x * ((double)hi + (double)lo); }
 __device__ __forceinline__ float2 mulk(float2 x, float hi, float lo) {
     return __ffma2_rn(make_float2(hi, hi), x, __fmul2_rn(make_float2(lo, lo), x));
 }
@@ -134,6 +136,34 @@ struct StoreF32 {
         __stcs(reinterpret_cast<float2*>(p), make_float2(v[0], v[1]));
     }
 };
+
+// FP64 storage and arithmetic: the reference runs the narrower forms are
+// measured against.  Plain values, no shift.
+struct StoreF64 {
+    using T = double;
+    static constexpr int kId = 3;
+    __device__ __forceinline__ static double ld(const T* p, int q, float r0) { return __ldg(p); }
+    __device__ __forceinline__ static void st(T* p, int q, float r0, double v) { __stcs(p, v); }
+    __device__ __forceinline__ static void ld2(const T* p, int q, float r0, double* o) {
+        const double2 v = *reinterpret_cast<const double2*>(p);
+        o[0] = v.x; o[1] = v.y;
+    }
+    __device__ __forceinline__ static void st2(T* p, int q, float r0, const double* v) {
+        __stcs(reinterpret_cast<double2*>(p), make_double2(v[0], v[1]));
+    }
+    __device__ __forceinline__ static void ld4(const T* p, int q, float r0, double* o) {
+        ld2(p, q, r0, o); ld2(p + 2, q, r0, o + 2);
+    }
+    __device__ __forceinline__ static void st4(T* p, int q, float r0, const double* v) {
+        st2(p, q, r0, v); st2(p + 2, q, r0, v + 2);
+    }
+};
+
+// arithmetic type of a storage form: FP32 for every form but FP64
+template <class ST> struct Real { using type = float; };
+template <> struct Real<StoreF64> { using type = double; };
+// the shifted narrow forms (F16, BF16), which compute in stored units
+template <class ST> constexpr bool kNarrow = ST::kId == 1 || ST::kId == 2;
 
 // F16 keeps the shifted value scaled by 2^10 (exact in FP32): |f - w rho0| < 64
 // fits, and deviations down to 6e-8 stay normal numbers instead of subnormals.
@@ -252,6 +282,16 @@ template <> struct Raw<StoreF16> {
     __device__ __forceinline__ static void st2(T* p, const float* v) {
         *reinterpret_cast<__half2*>(p) = __floats2half2_rn(v[0], v[1]);
     }
+    // stochastically rounded stores (rb: random bits, see cvt_rs_f16x2)
+    __device__ __forceinline__ static void st_sr(T* p, float g, uint32_t rb) {
+        __stcs(reinterpret_cast<unsigned short*>(p), (unsigned short)(cvt_rs_f16x2(g, 0.f, rb) & 0xffffu));
+    }
+    __device__ __forceinline__ static void st2_sr(T* p, const float* v, uint32_t rb) {
+        __stcs(reinterpret_cast<unsigned int*>(p), cvt_rs_f16x2(v[0], v[1], rb));
+    }
+    __device__ __forceinline__ static void st4_sr(T* p, const float* v, uint32_t rb0, uint32_t rb1) {
+        __stcs(reinterpret_cast<uint2*>(p), make_uint2(cvt_rs_f16x2(v[0], v[1], rb0), cvt_rs_f16x2(v[2], v[3], rb1)));
+    }
 };
 template <> struct Raw<StoreBF16> {
     using T = __nv_bfloat16;
@@ -280,7 +320,33 @@ template <> struct Raw<StoreBF16> {
     __device__ __forceinline__ static void st2(T* p, const float* v) {
         *reinterpret_cast<__nv_bfloat162*>(p) = __floats2bfloat162_rn(v[0], v[1]);
     }
+    __device__ __forceinline__ static void st_sr(T* p, float g, uint32_t rb) {
+        __stcs(reinterpret_cast<unsigned short*>(p), (unsigned short)(cvt_rs_bf16x2(g, 0.f, rb) & 0xffffu));
+    }
+    __device__ __forceinline__ static void st2_sr(T* p, const float* v, uint32_t rb) {
+        __stcs(reinterpret_cast<unsigned int*>(p), cvt_rs_bf16x2(v[0], v[1], rb));
+    }
+    __device__ __forceinline__ static void st4_sr(T* p, const float* v, uint32_t rb0, uint32_t rb1) {
+        __stcs(reinterpret_cast<uint2*>(p),
+               make_uint2(cvt_rs_bf16x2(v[0], v[1], rb0), cvt_rs_bf16x2(v[2], v[3], rb1)));
+    }
 };
+// Random words for the stochastically rounded stores of one thread: one hash of
+// the (global) index of its first cell and of a value it loaded, then a cheap
+// odd-multiplier derivation per stored word k (k < 64).
+__device__ __forceinline__ uint32_t sr_seed(uint32_t cell, float v) {
+    return mix32(cell ^ (__float_as_uint(v) * 0x9e3779b9u));
+}
+__device__ __forceinline__ uint32_t sr_word(uint32_t h, int k) {
+    uint32_t rb = h * ((2u * (uint32_t)k + 1u) * 0x85ebca6bu);
+    return rb ^ (rb >> 15);
+}
+template <class ST, int VEC>
+__device__ __forceinline__ void stv_raw_sr(typename ST::T* p, const float* v, uint32_t h, int q) {
+    if constexpr (VEC == 4) Raw<ST>::st4_sr(p, v, sr_word(h, 2 * q), sr_word(h, 2 * q + 1));
+    else if constexpr (VEC == 2) Raw<ST>::st2_sr(p, v, sr_word(h, 2 * q));
+    else Raw<ST>::st_sr(p, v[0], sr_word(h, 2 * q));
+}
 template <class ST, int VEC>
 __device__ __forceinline__ void ldv_raw(const typename ST::T* p, float* o) {
     if constexpr (VEC == 4) Raw<ST>::ld4(p, o);
@@ -295,13 +361,13 @@ __device__ __forceinline__ void stv_raw(typename ST::T* p, const float* v) {
 }
 
 template <class ST, int VEC>
-__device__ __forceinline__ void ldv(const typename ST::T* p, int q, float r0, float* o) {
+__device__ __forceinline__ void ldv(const typename ST::T* p, int q, float r0, typename Real<ST>::type* o) {
     if constexpr (VEC == 4) ST::ld4(p, q, r0, o);
     else if constexpr (VEC == 2) ST::ld2(p, q, r0, o);
     else o[0] = ST::ld(p, q, r0);
 }
 template <class ST, int VEC>
-__device__ __forceinline__ void stv(typename ST::T* p, int q, float r0, const float* v) {
+__device__ __forceinline__ void stv(typename ST::T* p, int q, float r0, const typename Real<ST>::type* v) {
     if constexpr (VEC == 4) ST::st4(p, q, r0, v);
     else if constexpr (VEC == 2) ST::st2(p, q, r0, v);
     else ST::st(p, q, r0, v[0]);

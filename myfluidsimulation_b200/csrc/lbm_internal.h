@@ -31,6 +31,7 @@ struct AAParams {
     // all N, or the interior planes of a z-slab whose first and last planes are
     // ghost copies of the neighbouring slabs' boundary planes
     int64_t first, cells;
+    uint32_t salt_base;      // F16/BF16 stochastic rounding: index of cell 0 in the whole grid
 };
 
 // Parameters of one HOME step (moment-only, two buffers).
@@ -80,6 +81,8 @@ cudaError_t launch_aa_materialize(const AAParams& p, int storage, int parity, fl
 // sets the dynamic shared-memory limit of the HOME kernels (call outside graph capture)
 cudaError_t home_prepare();
 int home_num_blocks(int nx, int ny, int nz, int zchunk);
+// resident HOME blocks per SM (occupancy of the FP32 step kernel)
+int home_blocks_per_sm();
 cudaError_t launch_home_step(const HomeParams& p, int storage, int tile_y, int blocks_per_sm, cudaStream_t s);
 // HOME moments (storage type) -> float 10*N
 cudaError_t launch_home_export(const void* m, int storage, int64_t N, float rho0, float* out, cudaStream_t s);

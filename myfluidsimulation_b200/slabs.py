@@ -29,7 +29,10 @@ import numpy as np
 from ._lib import BC_PERIODIC, METHOD_HOME, METHOD_LEGACY, STORE_F32, check, lib
 from .solvers import Solver
 
-__all__ = ["slab_bounds", "exchange_plan", "exchange", "with_ghosts", "SlabSet", "DistSlab"]
+__all__ = ["slab_bounds", "exchange_plan", "exchange", "with_ghosts", "reduce_stats", "SlabSet", "DistSlab"]
+
+# FP64 statistics of a solver, in the order of lbm_get_stats (LBM_STAT_* in lbm_capi.h)
+STAT_KEYS = ("mass", "ke_sum", "drag_x", "drag_y", "drag_z", "mom_x", "mom_y", "mom_z")
 
 
 def slab_bounds(nz: int, parts: int):
@@ -46,6 +49,21 @@ def with_ghosts(a, z0: int, z1: int, axis: int = 0):
     nz = a.shape[axis]
     idx = [(z0 - 1) % nz] + list(range(z0, z1)) + [z1 % nz]
     return np.ascontiguousarray(np.take(a, idx, axis=axis))
+
+
+def reduce_stats(local: dict, cells: int, dist, group=None) -> dict:
+    """The whole grid's statistics from every rank's own sums: one FP64
+    all-reduce (sum) of the 8 values over the group.  A slab's sums cover its
+    own planes only (ghost planes are never stepped), so the sum over the ranks
+    counts every cell once.  The tensor lives on the GPU for NCCL and on the
+    host for other backends (gloo)."""
+    import torch
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    v = torch.tensor([float(local[k]) for k in STAT_KEYS], dtype=torch.float64, device=dev)
+    dist.all_reduce(v, op=dist.ReduceOp.SUM, group=group)
+    out = dict(zip(STAT_KEYS, v.cpu().tolist()))
+    out["ke_mean"] = out["ke_sum"] / cells
+    return out
 
 
 # planes of a slab solver with L planes: 0 ghost below, 1 first own, L-2 last own, L-1 ghost above
@@ -333,6 +351,13 @@ class DistSlab:
 
     def synchronize(self):
         self.solver.synchronize()
+
+    def stats(self) -> dict:
+        """Mass, kinetic energy, momentum-exchange drag and momentum of the whole
+        grid (FP64, from the last step with statistics on): this rank's sums
+        over its own planes, added over the ranks by one FP64 all-reduce.  Every
+        rank must call it (a collective)."""
+        return reduce_stats(self.solver.stats(), int(np.prod(self.shape)), self.dist, self.group)
 
     def macros(self):
         """This rank's planes z0..z1-1 of rho, ux, uy, uz."""

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (BC_DUCT, BC_PERIODIC, BOUNCE_HALFWAY, BOUNCE_REFERENCE, METHOD_HOME, METHOD_HYBRID,
-                   METHOD_LEGACY, NSTAT, STORE_BF16, STORE_F16, STORE_F32, check, lib)
+                   METHOD_LEGACY, NSTAT, STORE_BF16, STORE_F16, STORE_F32, STORE_F64, check, lib)
 
 STAT_NAMES = ("mass", "ke_sum", "drag_x", "drag_y", "drag_z", "mom_x", "mom_y", "mom_z")
 
@@ -273,7 +273,7 @@ class LBM3D_Hybrid(_RefSolver):
 
 
 __all__ = ["Domain", "Solver", "LBM3D_Legacy", "LBM3D_Home", "LBM3D_Hybrid", "METHOD_LEGACY", "METHOD_HOME",
-           "METHOD_HYBRID", "STORE_F32", "STORE_F16", "STORE_BF16", "BC_PERIODIC", "BC_DUCT", "BOUNCE_HALFWAY",
+           "METHOD_HYBRID", "STORE_F32", "STORE_F16", "STORE_BF16", "STORE_F64", "BC_PERIODIC", "BC_DUCT", "BOUNCE_HALFWAY",
            "BOUNCE_REFERENCE"]
 
 

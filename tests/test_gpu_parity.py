@@ -415,3 +415,51 @@ def test_stats_async_equals_sync(gpu):
                                                                         "mom_x", "mom_y", "mom_z")]))
     assert not np.array_equal(got[0], got[-1])
     s.close()
+
+
+@pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HYBRID])
+@pytest.mark.parametrize("bc", [BC_PERIODIC, BC_DUCT])
+def test_f64_storage_vs_oracle(gpu, oracle, method, bc):
+    """FP64 storage and arithmetic (the reference form of the precision
+    measurements) against the FP64 oracle: the FP64 statistics agree to FP64
+    rounding (1e-11 relative over 20 steps), the FP32 read-out of the state to
+    FP32 rounding (1e-7)."""
+    from myfluidsimulation_b200.solvers import STORE_F64
+    dims = (40, 18, 14)
+    nx, ny, nz = dims
+    mask = obstacle_mask(*dims, seed=31, duct=bc == BC_DUCT)
+    fields = init_fields(*dims, seed=32)
+    band = oracle.band(mask, 2)[1] if method == METHOD_HYBRID else None
+    steps, tau, u_in = 20, 0.58, 0.04 if bc == BC_DUCT else 0.0
+    force = (1e-5, 0, 0) if bc == BC_PERIODIC else (0, 0, 0)
+    s = Solver(*dims, tau, force, method=method, storage=STORE_F64, bc=bc, inlet_u=u_in)
+    s.set_solid_mask(mask)
+    if band is not None:
+        s.set_legacy_mapping(band)
+        s.set_shear_omega(1.0 / 0.61)
+    s.reinit_from_host(*fields)
+    s.step(steps - 1)
+    s.enable_stats(True)
+    s.step(1)
+    s.synchronize()
+    st, state = s.stats(), s.state()
+    s.close()
+    # the solver's parameters are FP32 (omega = 1/tau in FP32, force, inlet
+    # speed): the oracle gets exactly those values
+    f32 = lambda x: float(np.float32(x))
+    tau_eff = 1.0 / float(np.float32(1.0) / np.float32(tau))
+    f0 = oracle.reinit_eq(*[np.float64(a) for a in fields])
+    f, r, u, v, w, drag = oracle.bgk_run(f0, mask, steps, tau_eff, tuple(f32(x) for x in force),
+                                        mode=1 if band is not None else 0, band=band,
+                                        omega_s=f32(1.0 / 0.61) if band is not None else None,
+                                        bc=1 if bc == BC_DUCT else 0, u_in=f32(u_in))
+    assert rl2(state, f) < 1e-7
+    fluid = mask == 0
+    mass = r[fluid].sum()
+    ke = 0.5 * (u * u + v * v + w * w)[fluid].sum()
+    mom = (r * u)[fluid].sum()
+    assert abs(st["mass"] - mass) <= 1e-11 * mass
+    assert abs(st["ke_sum"] - ke) <= 1e-11 * ke
+    assert abs(st["mom_x"] - mom) <= 1e-11 * np.abs(r * u)[fluid].sum()
+    if bc == BC_DUCT:
+        assert np.linalg.norm(np.array([st["drag_x"], st["drag_y"], st["drag_z"]]) - drag) <= 1e-11 * np.linalg.norm(drag)

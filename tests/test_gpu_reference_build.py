@@ -69,7 +69,7 @@ def run_ref(ref, method, dims, tau, fields, mask=None, steps=1, force=(0, 0, 0),
 @pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HOME])
 @pytest.mark.parametrize("steps", [1, 2, 25, 200])
 def test_tgv64_matches_reference_build(ref, method, steps):
-    """64^3 periodic Taylor-Green vortex, tau 0.6, u0 0.05."""
+    """The 64^3 periodic Taylor-Green vortex, tau 0.6, u0 0.05."""
     dims = (64, 64, 64)
     fields = W.taylor_green_3d(*dims, 0.05)
     (mr, mu, mv, mw), sm = run_mine(method, dims, 0.6, fields, steps=steps)

@@ -136,6 +136,28 @@ class _FakeDist:
     def get_world_size(self, group=None):
         return self.world
 
+    def get_backend(self, group=None):
+        return "gloo"
+
+    class ReduceOp:
+        SUM = "sum"
+
+    def all_reduce(self, t, op=None, group=None):
+        """Sum over the emulated ranks, added in rank order."""
+        k = self.nsend.get("ar", 0)
+        self.nsend["ar"] = k + 1
+        for r in range(self.world):
+            if r != self.rank:
+                self.mb.put(("ar", self.rank, r, k), t)
+        parts = {self.rank: t.clone()}
+        for r in range(self.world):
+            if r != self.rank:
+                parts[r] = self.mb.take(("ar", r, self.rank, k))
+        acc = parts[0].clone()
+        for r in range(1, self.world):
+            acc += parts[r]
+        t.copy_(acc)
+
     def isend(self, *a):
         raise AssertionError("used only as a P2POp tag")
 
@@ -176,7 +198,9 @@ def test_dist_slabs_equal_single_grid(gpu, oracle, world, method):
     if band is not None:
         one.set_legacy_mapping(band)
     one.reinit_from_host(*f)
-    one.step(10)
+    one.step(9)
+    one.enable_stats(True)
+    one.step(1)
     one.synchronize()
     box = _Mailbox()
     out, errs = {}, []
@@ -188,9 +212,11 @@ def test_dist_slabs_equal_single_grid(gpu, oracle, world, method):
             if band is not None:
                 d.set_legacy_mapping(band)
             d.reinit_from_host(*f)
-            d.step(10)
+            d.step(9)
+            d.enable_stats(True)
+            d.step(1)
             d.synchronize()
-            out[r] = (d.state(), d.macros())
+            out[r] = (d.state(), d.macros(), d.stats())
             d.close()
         except Exception as e:   # reported by the main thread
             errs.append(e)
@@ -206,6 +232,12 @@ def test_dist_slabs_equal_single_grid(gpu, oracle, world, method):
     mac = [np.concatenate([out[r][1][k] for r in range(world)], axis=0) for k in range(4)]
     for a, b in zip(mac, one.macros()):
         np.testing.assert_array_equal(a, b)
+    # the FP64 statistics: every rank's own sums, added over the ranks
+    want = one.stats()
+    for r in range(world):
+        got = out[r][2]
+        for k in ("mass", "ke_sum", "mom_x", "mom_y", "mom_z", "drag_x", "drag_y", "drag_z"):
+            assert abs(got[k] - want[k]) <= 1e-12 * max(abs(want[k]), abs(want["mass"]) * 1e-6), (k, got[k], want[k])
     assert [b for b in slab_bounds(nz, world)][-1][1] == nz
     one.close()
 

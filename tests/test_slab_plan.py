@@ -14,7 +14,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from myfluidsimulation_b200.slabs import exchange, exchange_plan, slab_bounds, with_ghosts
+from myfluidsimulation_b200.slabs import STAT_KEYS, exchange, exchange_plan, reduce_stats, slab_bounds, with_ghosts
 
 UP = [q for q in range(19) if q in (5, 11, 12, 15, 16)]     # c_z = +1
 DOWN = [q for q in range(19) if q in (6, 13, 14, 17, 18)]   # c_z = -1
@@ -92,3 +92,36 @@ def test_plan_pairs_and_bounds():
     a = np.arange(5 * 2).reshape(5, 2)
     np.testing.assert_array_equal(with_ghosts(a, 0, 2), a[[4, 0, 1, 2]])
     np.testing.assert_array_equal(with_ghosts(a, 3, 5), a[[2, 3, 4, 0]])
+
+
+def _stats_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        local = {k: (rank + 1) * 10.0 ** i + 0.125 * i for i, k in enumerate(STAT_KEYS)}
+        out[rank] = reduce_stats(local, 1000, dist)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_reduce_stats_sums_over_ranks(world):
+    """The slabs' FP64 statistics all-reduce as gloo ranks: every rank gets the
+    sum of all ranks' values, and the mean energy over the whole grid."""
+    ctx = mp.get_context("spawn")
+    mgr = ctx.Manager()
+    out = mgr.dict()
+    port = 29650 + world
+    procs = [ctx.Process(target=_stats_worker, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    for r in range(world):
+        got = out[r]
+        for i, k in enumerate(STAT_KEYS):
+            want = sum((q + 1) * 10.0 ** i + 0.125 * i for q in range(world))
+            assert got[k] == want
+        assert got["ke_mean"] == got["ke_sum"] / 1000

@@ -22,7 +22,9 @@ periodic workload, `*_inlet` for the inlet duct).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 With --gpus N (under torchrun) every rank runs its own duct instance (weak
-scaling, no data-path collective); time is the max over ranks.
+scaling, no data-path collective); time is the max over ranks.  With
+--decomp zslab the ranks instead hold z-slabs of ONE duct of 128 x N planes
+and exchange their face slots around every odd step through NCCL.
 --impl reference times the reference's own CUDA solvers (compiled from its
 sources into oracle/_ref) on the periodic workload, Legacy, HOME and
 Hybrid(B0=2), with the mask built by the reference's own STL loader and
@@ -983,6 +985,97 @@ def profile_tgv(args, torch):
                       "steps": 6}))
 
 
+def decomp_run(args, torch, dist, rank, world):
+    """The periodic duct stretched along z to 128 x N planes and split into N
+    z-slabs, one per rank (DistSlab: ghost planes, the 5 crossing slot planes of
+    each face exchanged point to point through NCCL around every odd step,
+    overlapped with the slab's interior planes).  Weak scaling: 128 planes per
+    GPU.  One bench step = 50 LBM steps, the last one with the FP64 statistics
+    all-reduced over the ranks."""
+    from myfluidsimulation_b200.slabs import DistSlab
+    from myfluidsimulation_b200.solvers import METHOD_LEGACY
+    W = load_workloads()
+    nzg = NZ * world
+    with tempfile.TemporaryDirectory() as td:
+        box, ntri, nsph = build_mask(td)          # one 256x128x128 box: walls + sphere
+    sphere = (box != 0) & (W.duct_mask(NX, NY, NZ) == 0)
+    obstacle = np.zeros((nzg, NY, NX), np.uint8)
+    obstacle[:NZ][sphere] = 1
+    mask = W.duct_mask(NX, NY, nzg, obstacle)
+    rho = np.ones(mask.shape, np.float32)
+    zero = np.zeros(mask.shape, np.float32)
+    d = DistSlab(NX, NY, nzg, TAU, FORCE, method=METHOD_LEGACY, dist=dist if world > 1 else _SoloDist())
+    d.set_solid_mask(mask)
+    d.reinit_from_host(rho, zero, None, None)
+    d.enable_stats(True)
+    st = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        d.step(DRAG_EVERY, overlap=True)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        e0.record(st)
+        for _ in range(args.steps):
+            d.step(DRAG_EVERY, overlap=True)
+        e1.record(st)
+        torch.cuda.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1)], device="cuda")
+    if dist:
+        dist.barrier()
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms = float(ms.item())
+    stats = d.stats()
+    d.close()
+    N = NX * NY * nzg
+    mlups = N * DRAG_EVERY * args.steps / (ms * 1e-3) / 1e6
+    per_launch = ms / (DRAG_EVERY * args.steps)
+    peak, peak_kind = measured_peaks()
+    achieved = NX * NY * NZ * BYTES["legacy"] / (per_launch * 1e-3) / 1e9
+    if rank == 0:
+        print(json.dumps({
+            "metric": METRIC, "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"periodic duct {NX}x{NY}x{nzg} (128 planes per GPU), y/z walls as solid cells, "
+                                   "icosphere r=16 at (64,64,64), x periodic, body force (1e-5,0,0), tau 0.56; "
+                                   "one step = 50 LBM steps + FP64 statistics all-reduced",
+                       "method": "legacy", "storage": "f32", "l2": HEAD_CONFIG["l2"],
+                       "parallelism": f"zslab x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None, "kernel": "aa_even/aa_odd per GPU",
+                         "bytes_per_cell": BYTES["legacy"], "peak_kind": peak_kind},
+            "exchange": {"bytes_per_face_per_odd_step": 2 * 5 * NX * NY * 4,
+                         "transport": "NCCL point to point, overlapped with interior planes" if world > 1 else
+                                      "self-exchange (one slab, device copies)"},
+            # per step pair: the even and odd kernels (3 parts each when overlapped) and the
+            # 10 merge kernels of phase 1; plus the statistics' final pass per bench step
+            "gpu_launches": args.steps * ((DRAG_EVERY // 2) * (16 if world > 1 else 12) + 1),
+            "stats": {"mass": stats["mass"], "drag": [stats["drag_x"], stats["drag_y"], stats["drag_z"]]},
+            "clocks": clk.summary()}))
+
+
+class _SoloDist:
+    """The torch.distributed calls a one-rank DistSlab makes, without a process group."""
+
+    def get_rank(self, group=None):
+        return 0
+
+    def get_world_size(self, group=None):
+        return 1
+
+    def get_backend(self, group=None):
+        return "gloo"
+
+    class ReduceOp:
+        SUM = "sum"
+
+    def all_reduce(self, t, op=None, group=None):
+        return None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -993,6 +1086,9 @@ def main():
                     help="comma list of run keys: legacy, home, hybrid (periodic workload), *_inlet (inlet duct); "
                          "the first is the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--decomp", default=None, choices=["zslab"],
+                    help="zslab: one periodic duct of 128 x N planes split into z-slabs over the N ranks "
+                         "(NCCL face exchange overlapped with the interior planes) instead of N replicas")
     ap.add_argument("--profile", default=None,
                     help="set up one run key (e.g. legacy, home_inlet) on the duct, or 'tgv' (the periodic "
                          "Taylor-Green vortex of --profile-n^3 cells, Legacy, --profile-storage), and run 4 LBM "
@@ -1045,6 +1141,12 @@ def main():
         return
     if args.profile == "tgv":
         profile_tgv(args, torch)
+        return
+    if args.decomp == "zslab":
+        decomp_run(args, torch, dist, rank, world)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
         return
     with tempfile.TemporaryDirectory() as td:
         mask, ntri, nsph = build_mask(td)

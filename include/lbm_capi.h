@@ -419,6 +419,14 @@ int lbm_zslab_exchange(lbm_solver* lower, lbm_solver* upper, int phase, void* st
  * values its cells wrote: every cell whose link towards that neighbour
  * streams (a cell that bounced its own population back keeps it). */
 int lbm_zslab_merge(lbm_solver* s, int plane, int cz, void* const* src, void* stream);
+/* One step of a z-slab solver over its planes [z_begin, z_end) only
+ * (1 <= z_begin <= z_end <= nz-1), so that the planes next to the ghosts can
+ * wait for an exchange while the interior computes: Legacy/Hybrid the current
+ * parity's kernel, HOME the moment step.  No statistics and no macro fields
+ * (use lbm_step for a step that writes them).  finish != 0 ends the step after
+ * this part: the parity flips (HOME: the buffers swap) and the step counts.
+ * No reference counterpart. */
+int lbm_zslab_step_planes(lbm_solver* s, int z_begin, int z_end, int finish);
 /* Every face of a periodic chain of n slabs (slab k below slab k+1, the last
  * below the first) in ONE launch per phase: the transfers of lbm_zslab_exchange
  * for all faces, as a job table built once.  The slabs' buffers must stay in

@@ -138,6 +138,7 @@ _PROTOS = [
     ("lbm_zslab_merge", C.c_int, [_P, C.c_int, C.c_int, C.POINTER(_P), _P]),
     ("lbm_zslab_moment_planes", C.c_int, [_P, C.c_int, C.POINTER(_P), C.POINTER(C.c_int64)]),
     ("lbm_set_index_base", C.c_int, [_P, C.c_int64]),
+    ("lbm_zslab_step_planes", C.c_int, [_P, C.c_int, C.c_int, C.c_int]),
     ("lbm_zslab_plan_create", C.c_int, [C.POINTER(_P), C.c_int32, C.POINTER(_P)]),
     ("lbm_zslab_plan_exchange", C.c_int, [_P, C.c_int, _P]),
     ("lbm_zslab_plan_destroy", C.c_int, [_P]),

@@ -749,6 +749,44 @@ int lbm_zslab_moment_planes(lbm_solver* s, int plane, void** ptrs, int64_t* byte
     return LBM_OK;
 }
 
+int lbm_zslab_step_planes(lbm_solver* s, int z_begin, int z_end, int finish) {
+    if (!s) { set_error("lbm_zslab_step_planes: null solver"); return LBM_ERR_INVALID; }
+    if (!s->zghost) { set_error("lbm_zslab_step_planes: a z-slab solver (lbm_set_z_ghosts) only"); return LBM_ERR_INVALID; }
+    if (is_ref_push(s)) { set_error("lbm_zslab_step_planes: not for the reference bounce table"); return LBM_ERR_UNSUPPORTED; }
+    if (z_begin < 1 || z_end > s->dom.nz - 1 || z_begin > z_end) {
+        set_error("lbm_zslab_step_planes: planes must satisfy 1 <= z_begin <= z_end <= nz-1");
+        return LBM_ERR_INVALID;
+    }
+    if (z_end > z_begin) {
+        if (is_aa(s)) {
+            lbm::AAParams p = aa_params(s, false, false);
+            const int64_t plane = (int64_t)s->dom.nx * s->dom.ny;
+            p.first = (int64_t)z_begin * plane;
+            p.cells = (int64_t)(z_end - z_begin) * plane;
+            CK(lbm::launch_aa_step(p, s->storage, s->parity, s->parity == 0 ? s->cfg_even : s->cfg_odd, s->stream));
+        } else {
+            const int rc = wait_pending_read(s);   // HOME's buffers are its macro fields
+            if (rc != LBM_OK) return rc;
+            lbm::HomeParams p = home_params(s, false);
+            p.zb = z_begin;
+            p.ze = z_end;
+            CK(lbm::launch_home_step(p, s->storage, 8, 3, s->stream));
+        }
+    }
+    if (finish) {
+        if (is_aa(s)) {
+            s->parity ^= 1;
+        } else {
+            s->cur ^= 1;
+            if (s->storage != LBM_STORE_F32)
+                CK(lbm::launch_home_macros(s->m[s->cur], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
+                                           s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
+        }
+        s->steps += 1;
+    }
+    return LBM_OK;
+}
+
 int lbm_set_index_base(lbm_solver* s, int64_t base) {
     if (!s) { set_error("lbm_set_index_base: null solver"); return LBM_ERR_INVALID; }
     s->salt_base = (uint32_t)(uint64_t)base;

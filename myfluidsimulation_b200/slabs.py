@@ -82,11 +82,14 @@ def exchange_plan(phase: int, rank: int, world: int):
     raise ValueError("phase is 0 or 1")
 
 
-def exchange(views, phase: int, rank: int, world: int, dist, group=None, recv_views=None):
+def exchange(views, phase: int, rank: int, world: int, dist, group=None, recv_views=None, wait=True):
     """Run one phase of the plan with torch.distributed point-to-point ops.
     views[(plane, cz)]: the 5 tensors (slot planes) of that plane and
     direction set, in direction order, on this rank; recv_views (optional)
-    redirects receives of a (plane, cz) into other tensors (staging)."""
+    redirects receives of a (plane, cz) into other tensors (staging).
+    wait=False returns the works instead of waiting for them (with NCCL, a
+    work's wait() makes the current stream wait: the transfers overlap with
+    whatever the stream runs until then)."""
     ops = []
     for kind, peer, plane, cz in exchange_plan(phase, rank, world):
         fn = dist.isend if kind == "send" else dist.irecv
@@ -96,8 +99,12 @@ def exchange(views, phase: int, rank: int, world: int, dist, group=None, recv_vi
             ts = recv_views[(plane, cz)]
         for t in ts:
             ops.append(dist.P2POp(fn, t, peer_g, group))
-    for w in dist.batch_isend_irecv(ops):
+    works = dist.batch_isend_irecv(ops)
+    if not wait:
+        return works
+    for w in works:
         w.wait()
+    return []
 
 
 def _slot_ptrs(solver: Solver, plane: int, cz: int):
@@ -278,6 +285,7 @@ class DistSlab:
         self.planes = planes
         self.views = {}
         self._home_views = {}
+        self._pending = []          # phase-1 works of an overlapped odd step, merged before the next use
         if not self.home:
             for name, pl in planes.items():
                 for cz in (+1, -1):
@@ -307,6 +315,49 @@ class DistSlab:
             self._home_views[key] = v
         return self._home_views[key]
 
+    def _merge_staging(self):
+        for (name, cz), ts in self.staging.items():
+            src = (C.c_void_p * 5)(*[t.data_ptr() for t in ts])
+            check(lib().lbm_zslab_merge(self.solver._h, self.planes[name], cz, src,
+                                        C.c_void_p(self.solver.stream)))
+
+    def _flush(self):
+        """Complete a phase-1 exchange left in flight by an overlapped odd step."""
+        if self._pending:
+            for w in self._pending:
+                w.wait()
+            self._pending = []
+            self._merge_staging()
+
+    def _planes(self, z0, z1, finish):
+        check(lib().lbm_zslab_step_planes(self.solver._h, int(z0), int(z1), 1 if finish else 0))
+
+    def _step_overlapped(self):
+        """One step with the face exchange overlapped with the interior planes
+        (Legacy/Hybrid, 2 or more ranks, at least 3 own planes).  In the AA
+        pattern every cell reads exactly the slots it writes, so planes can be
+        stepped in any order.  Odd step: phase 0 goes out, the interior planes
+        2..L-3 compute meanwhile (they touch neither the ghost planes nor the
+        boundary slots that phase 0 sends), then the two boundary planes; phase 1
+        is left in flight.  Even step: the interior computes while phase 1
+        lands, then the merge and the two boundary planes."""
+        L = self.planes["ghost_hi"] + 1
+        if _parity(self.solver) == 1:
+            self._flush()
+            works = exchange(self.views, 0, self.rank, self.world, self.dist, self.group, wait=False)
+            self._planes(2, L - 2, False)
+            for w in works:
+                w.wait()
+            self._planes(1, 2, False)
+            self._planes(L - 2, L - 1, True)
+            self._pending = exchange(self.views, 1, self.rank, self.world, self.dist, self.group,
+                                     recv_views=self.staging, wait=False)
+        else:
+            self._planes(2, L - 2, False)
+            self._flush()
+            self._planes(1, 2, False)
+            self._planes(L - 2, L - 1, True)
+
     def _exchange(self, phase):
         if self.world == 1:
             check(lib().lbm_zslab_exchange(self.solver._h, self.solver._h, phase, C.c_void_p(self.solver.stream)))
@@ -319,10 +370,7 @@ class DistSlab:
             exchange(self.views, 0, self.rank, self.world, self.dist, self.group)
             return
         exchange(self.views, 1, self.rank, self.world, self.dist, self.group, recv_views=self.staging)
-        for (name, cz), ts in self.staging.items():
-            src = (C.c_void_p * 5)(*[t.data_ptr() for t in ts])
-            check(lib().lbm_zslab_merge(self.solver._h, self.planes[name], cz, src,
-                                        C.c_void_p(self.solver.stream)))
+        self._merge_staging()
 
     def set_solid_mask(self, mask):
         self.solver.set_solid_mask(with_ghosts(np.asarray(mask, np.uint8).reshape(self.shape), self.z0, self.z1))
@@ -334,8 +382,17 @@ class DistSlab:
         self.solver.reinit_from_host(*[None if a is None else with_ghosts(
             np.asarray(a, np.float32).reshape(self.shape), self.z0, self.z1) for a in (rho, ux, uy, uz)])
 
-    def step(self, n: int = 1):
-        for _ in range(n):
+    def step(self, n: int = 1, overlap: bool = False):
+        """n steps.  overlap=True overlaps the face exchange with the interior
+        planes (Legacy/Hybrid on 2 or more ranks, 3 or more own planes) for every
+        step but the last, which runs whole, so that its statistics and macro
+        fields come out as from lbm_step."""
+        can = overlap and not self.home and self.world > 1 and self.planes["ghost_hi"] - 1 >= 3
+        for k in range(n):
+            if can and k < n - 1:
+                self._step_overlapped()
+                continue
+            self._flush()
             ex = self.home or _parity(self.solver) == 1
             if ex:
                 self._exchange(0)
@@ -350,6 +407,7 @@ class DistSlab:
         self.solver.enable_stats(on)
 
     def synchronize(self):
+        self._flush()
         self.solver.synchronize()
 
     def stats(self) -> dict:
@@ -357,15 +415,19 @@ class DistSlab:
         grid (FP64, from the last step with statistics on): this rank's sums
         over its own planes, added over the ranks by one FP64 all-reduce.  Every
         rank must call it (a collective)."""
+        self._flush()
         return reduce_stats(self.solver.stats(), int(np.prod(self.shape)), self.dist, self.group)
 
     def macros(self):
         """This rank's planes z0..z1-1 of rho, ux, uy, uz."""
+        self._flush()
         return tuple(m[1:-1] for m in self.solver.macros())
 
     def state(self):
         """This rank's populations (natural layout after an even step count)."""
+        self._flush()
         return self.solver.state()[:, 1:-1]
 
     def close(self):
+        self._flush()
         self.solver.close()

@@ -182,10 +182,14 @@ class _FakeDist:
         return [self._Work() for _ in ops]
 
 
-@pytest.mark.parametrize("world,method", [(2, METHOD_LEGACY), (3, METHOD_HYBRID), (3, METHOD_HOME)])
-def test_dist_slabs_equal_single_grid(gpu, oracle, world, method):
+@pytest.mark.parametrize("world,method,overlap", [(2, METHOD_LEGACY, False), (3, METHOD_HYBRID, False),
+                                                  (3, METHOD_HOME, False), (2, METHOD_LEGACY, True),
+                                                  (3, METHOD_HYBRID, True)])
+def test_dist_slabs_equal_single_grid(gpu, oracle, world, method, overlap):
     """DistSlab's multi-rank path (views of the slot planes, point-to-point plan,
-    staging and merge) with `world` ranks emulated by threads on this GPU."""
+    staging and merge) with `world` ranks emulated by threads on this GPU; with
+    overlap, the steps that split each slab into interior and boundary planes
+    around the exchange (lbm_zslab_step_planes)."""
     import threading
     from myfluidsimulation_b200.slabs import DistSlab, slab_bounds
     nx, ny, nz = 32, 18, 27
@@ -212,7 +216,7 @@ def test_dist_slabs_equal_single_grid(gpu, oracle, world, method):
             if band is not None:
                 d.set_legacy_mapping(band)
             d.reinit_from_host(*f)
-            d.step(9)
+            d.step(9, overlap=overlap)
             d.enable_stats(True)
             d.step(1)
             d.synchronize()

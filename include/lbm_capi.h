@@ -212,8 +212,10 @@ int lbm_get_stats_async(lbm_solver* s, double* out);
 /* Enables (1, the default) or disables (0) the macro-field output of
  * Legacy/Hybrid steps.  Disabled, lbm_step writes only the populations (the
  * macro buffers keep their last values), which saves 16 B per cell on the
- * last substep; statistics, when enabled, still write them.  HOME's macro
- * fields are its state and are always current. */
+ * last substep; statistics, when enabled, still write them.  HOME F32's macro
+ * fields are its state and are always current; HOME in F16/BF16/F64 exports
+ * them to FP32 after each lbm_step while the output is on, and otherwise when
+ * lbm_macro_ptrs, lbm_get_macros or lbm_read_macros_async next asks for them. */
 int lbm_set_macro_output(lbm_solver* s, int enable);
 
 /* Captures `substeps` steps into a CUDA graph on first use and replays it;

@@ -78,6 +78,9 @@ struct lbm_solver {
     cudaEvent_t ev_staged[2] = {nullptr, nullptr}, ev_stage_free[2] = {nullptr, nullptr};
     cudaEvent_t ev_macros = nullptr, ev_read = nullptr;
     bool read_pending = false;
+    // HOME F16/BF16/F64: the FP32 macro fields are exported from the state after
+    // each lbm_step while macro output is on, else when they are next asked for
+    bool macros_stale = false;
 };
 
 namespace {
@@ -108,6 +111,29 @@ int home_planes(const lbm_solver* s) { return s->zghost ? s->dom.nz - 2 : s->dom
 float* home_macro_base(lbm_solver* s) {
     // F32 HOME exposes its state directly (d_rho() = m + 0*N, home.cu:355-362)
     return s->storage == LBM_STORE_F32 ? static_cast<float*>(s->m[s->cur]) : s->macro;
+}
+
+// the macro fields of the current state: AA writes them in the step; HOME in
+// another storage than F32 exports them (now, or when they were skipped)
+int macro_fields(lbm_solver* s, float** base) {
+    if (is_aa(s)) { *base = s->macro; return LBM_OK; }
+    if (s->storage != LBM_STORE_F32 && s->macros_stale) {
+        CK(lbm::launch_home_macros(s->m[s->cur], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
+                                   s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
+        s->macros_stale = false;
+    }
+    *base = home_macro_base(s);
+    return LBM_OK;
+}
+
+// after a HOME step in another storage than F32: export the macro fields now
+// when macro output is on, else mark them for export on demand
+int home_after_step(lbm_solver* s) {
+    if (is_aa(s) || s->storage == LBM_STORE_F32) return LBM_OK;
+    s->macros_stale = true;
+    if (!s->macro_out) return LBM_OK;
+    float* b = nullptr;
+    return macro_fields(s, &b);
 }
 
 int rebuild_flags(lbm_solver* s) {
@@ -210,9 +236,10 @@ static int enqueue_steps(lbm_solver* s, int n) {
         }
         if (st) CK(lbm::launch_finalize_stats(s->partials, s->last_stat_blocks, s->stats, s->stream));
     }
-    if (!is_aa(s) && s->storage != LBM_STORE_F32 && n > 0)
-        CK(lbm::launch_home_macros(s->m[s->cur], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
-                                   s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
+    if (n > 0) {
+        const int rc = home_after_step(s);
+        if (rc != LBM_OK) return rc;
+    }
     s->steps += n;
     return LBM_OK;
 }
@@ -493,9 +520,11 @@ static int reinit_impl(lbm_solver* s, const float* d_rho, const float* d_ux, con
     } else {
         CK(lbm::launch_home_reinit(s->m[0], s->m[1], s->storage, s->rho0, s->N, d_rho, d_ux, d_uy, d_uz, s->stream));
         s->cur = 0;
-        if (s->storage != LBM_STORE_F32)
+        if (s->storage != LBM_STORE_F32) {
+            s->macros_stale = false;
             CK(lbm::launch_home_macros(s->m[0], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
                                        s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
+        }
     }
     s->steps = 0;
     drop_graph(s);
@@ -590,7 +619,8 @@ int lbm_read_macros_async(lbm_solver* s, float* rho, float* ux, float* uy, float
     if (rc != LBM_OK) return rc;
     rc = wait_pending_read(s);   // one read in flight at a time
     if (rc != LBM_OK) return rc;
-    float* b = is_aa(s) ? s->macro : home_macro_base(s);
+    float* b = nullptr;
+    if ((rc = macro_fields(s, &b)) != LBM_OK) return rc;
     CK(cudaEventRecord(s->ev_macros, s->stream));
     CK(cudaStreamWaitEvent(s->copy_stream, s->ev_macros, 0));
     float* dst[4] = {rho, ux, uy, uz};
@@ -649,6 +679,7 @@ int lbm_step_graph(lbm_solver* s, int substeps) {
     // advance the host-side state exactly as enqueue_steps would
     if (is_aa(s)) s->parity ^= (substeps & 1);
     else s->cur ^= (substeps & 1);
+    if (!is_aa(s) && s->storage != LBM_STORE_F32) s->macros_stale = !s->macro_out;
     s->steps += substeps;
     return LBM_OK;
 }
@@ -778,9 +809,8 @@ int lbm_zslab_step_planes(lbm_solver* s, int z_begin, int z_end, int finish) {
             s->parity ^= 1;
         } else {
             s->cur ^= 1;
-            if (s->storage != LBM_STORE_F32)
-                CK(lbm::launch_home_macros(s->m[s->cur], s->storage, s->N, s->rho0, s->macro, s->macro + s->N,
-                                           s->macro + 2 * s->N, s->macro + 3 * s->N, s->stream));
+            const int rc = home_after_step(s);
+            if (rc != LBM_OK) return rc;
         }
         s->steps += 1;
     }
@@ -954,7 +984,9 @@ int lbm_home_zchunk(lbm_solver* s, int* zchunk) {
 
 int lbm_macro_ptrs(lbm_solver* s, float** d_rho, float** d_u, float** d_v, float** d_w) {
     if (!s) { set_error("lbm_macro_ptrs: null solver"); return LBM_ERR_INVALID; }
-    float* b = is_aa(s) ? s->macro : home_macro_base(s);
+    float* b = nullptr;
+    const int rc = macro_fields(s, &b);
+    if (rc != LBM_OK) return rc;
     if (d_rho) *d_rho = b;
     if (d_u) *d_u = b + s->N;
     if (d_v) *d_v = b + 2 * s->N;
@@ -964,7 +996,9 @@ int lbm_macro_ptrs(lbm_solver* s, float** d_rho, float** d_u, float** d_v, float
 
 int lbm_get_macros(lbm_solver* s, float* rho, float* ux, float* uy, float* uz) {
     if (!s) { set_error("lbm_get_macros: null solver"); return LBM_ERR_INVALID; }
-    float* b = is_aa(s) ? s->macro : home_macro_base(s);
+    float* b = nullptr;
+    const int rc = macro_fields(s, &b);
+    if (rc != LBM_OK) return rc;
     float* dst[4] = {rho, ux, uy, uz};
     for (int k = 0; k < 4; ++k)
         if (dst[k]) CK(cudaMemcpyAsync(dst[k], b + k * s->N, sizeof(float) * (size_t)s->N, cudaMemcpyDeviceToHost, s->stream));

@@ -40,6 +40,27 @@ TOL = {STORE_F32: dict(drag=3e-4, rho=1e-5, u=1e-4), STORE_F64: dict(drag=1e-9, 
 _oracle_runs = {}
 
 
+def rl2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+@pytest.fixture(scope="module")
+def duct_mask(gpu):
+    nx, ny, nz = DIMS
+    tris, scale, tr = W.duct_sphere_mesh(nx, ny, nz, 16, (64, 64, 64))
+    sph = G.voxelize_mesh_to_mask(G.mesh_from_triangles(tris), G.VoxelParams(nx, ny, nz, scale, tr))
+    return W.duct_mask(nx, ny, nz, sph)
+
+
+def _inlet_fields(mask):
+    rho = np.ones(mask.shape, np.float32)
+    u = np.full(mask.shape, U_IN, np.float32)
+    u[mask != 0] = 0
+    return rho, u
+
+
 def _oracle_inlet(oracle, method, mask, rho, u, band):
     """The FP64 oracle on the inlet duct: drag after every chunk, fields at the end
     (kept for the FP32 and FP64 cases of the same method)."""

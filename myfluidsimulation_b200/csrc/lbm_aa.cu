@@ -324,12 +324,27 @@ struct Nbr {
     __device__ __forceinline__ IDX at(int dx, int dy, int dz) const { return r[dy + 1][dz + 1] + xs[dx + 1]; }
 };
 
+// Element offsets of the 19 population planes, for the odd step's gathers
+// (plane opp(q)) and scatters (plane q), computed once per launch (or unit).
+template <class IDX>
+struct PlaneOffs {
+    IDX g[19], s[19];
+    __device__ __forceinline__ void init(IDX N) {
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            g[q] = (IDX)opp(q) * N;
+            s[q] = (IDX)q * N;
+        }
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Odd step
 // ---------------------------------------------------------------------------
 // One odd-step cell: x of row `row` (= z*ny + y).
 template <class ST, bool MASK, int MODE, class IDX>
-__device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, double (&acc)[NSTAT]) {
+__device__ __forceinline__ void odd_cell(const AAParams& p, const PlaneOffs<IDX>& po, IDX row, int x,
+                                         double (&acc)[NSTAT]) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     constexpr bool SH = kNarrow<ST>;    // narrow forms: compute in stored units
     using T = typename ST::T;
@@ -357,7 +372,7 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, doub
             // incoming q travels the link x -> x + c_opp(q); if that link does not
             // stream, the value was left in the cell's own slot q
             const bool nn = (lk >> opp(q)) & 1u;
-            const IDX src = nn ? ((IDX)q * N + id) : ((IDX)opp(q) * N + nb.at(-cx(q), -cy(q), -cz(q)));
+            const IDX src = nn ? (po.s[q] + id) : (po.g[q] + nb.at(-cx(q), -cy(q), -cz(q)));
             if constexpr (SH) c[q] = Raw<ST>::ld(f + src);
             else c[q] = ST::ld(f + src, q, p.rho0);
         }
@@ -383,7 +398,7 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, IDX row, int x, doub
                 if (cx(q) < 0) v = (nn && at_in) ? inlet_value(q, m.r, kin) : v;
             }
             if (cx(q) > 0) v = (nn && at_out) ? o[opp(q)] : v;
-            const IDX dst = nn ? ((IDX)opp(q) * N + id) : ((IDX)q * N + nb.at(cx(q), cy(q), cz(q)));
+            const IDX dst = nn ? (po.g[q] + id) : (po.s[q] + nb.at(cx(q), cy(q), cz(q)));
             if constexpr (SH) Raw<ST>::st_sr(f + dst, v, sr_word(hsr, 2 * q));
             else ST::st(f + dst, q, p.rho0, v);
         }
@@ -409,10 +424,12 @@ __global__ void __launch_bounds__(256, ST::kId == 3 ? 2 : (MASK ? 4 : 3)) aa_odd
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
+    PlaneOffs<IDX> po;
+    po.init((IDX)p.N);
     for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
         const IDX row = row0 + sg / segs;
         const int x = (int)(sg - (sg / segs) * segs) * bx + threadIdx.x;
-        if (x < p.nx) odd_cell<ST, MASK, MODE, IDX>(p, row, x, acc);
+        if (x < p.nx) odd_cell<ST, MASK, MODE, IDX>(p, po, row, x, acc);
     }
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }
@@ -548,10 +565,12 @@ __global__ void __launch_bounds__(256, 4) aa_batch_odd(const AAParams* __restric
         double acc[NSTAT];
 #pragma unroll
         for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
+        PlaneOffs<uint32_t> po;
+        po.init((uint32_t)p.N);
         // consecutive cells across row ends, so narrow rows leave no thread idle
         for (int c = w.y + (int)threadIdx.x; c < w.y + w.z; c += (int)blockDim.x) {
             const int row = c / p.nx;
-            odd_cell<ST, true, MODE, uint32_t>(p, (uint32_t)row, c - row * p.nx, acc);
+            odd_cell<ST, true, MODE, uint32_t>(p, po, (uint32_t)row, c - row * p.nx, acc);
         }
         if constexpr (STATS) block_reduce_into(acc, partials + (size_t)u * NSTAT);
     }

@@ -48,15 +48,7 @@ constexpr int TX = 32;                 // tile width (cells), 16 pairs
 constexpr int TY = 8;                  // tile height (rows)
 constexpr int NCW = TY / 2;            // tile warps: two rows of 16 pairs each
 constexpr int NT = (NCW + 2) * 32;     // + the halo-row warp + the halo-column warp
-// One ring plane (one population, one slot) holds rows y = -1..TY and columns
-// x = -2..TX+1 of the tile, pitch TX + 4 = 36 words.  The margins take the
-// writes whose destination lies outside the tile (nobody reads them), so the
-// tile's writes need no test, and with a 36-word pitch the 8 rows of one column
-// fall in 8 different banks.
-constexpr int PITCH = TX + 4;
-constexpr int ROWS = TY + 2;
-constexpr int PL = PITCH * ROWS;       // positions per population plane of the ring
-__host__ __device__ constexpr int rpos(int x, int y) { return (y + 1) * PITCH + x + 2; }
+constexpr int PL = TX * TY;            // positions per population plane of the ring
 
 // shared ring (destination-indexed), grouped by c_z: UP[3][5][PL], MID[2][9][PL], DN[5][PL]
 constexpr int UP_SZ = 5 * PL, MID_SZ = 9 * PL, DN_SZ = 5 * PL;
@@ -329,30 +321,31 @@ __device__ __forceinline__ void store_pair(T* op, IDX N, float r0, const V (&out
     }
 }
 
-// Ring writes of a source pair, population q: its two cells' values go to the
-// ring positions of the pair's own first and second cell shifted by c_q
-// (destination (x + c_x, y + c_y)).  A pair that stays in x is one aligned
-// 8-byte store at the first cell's position pos.  A shifted pair is two 4-byte stores; the
-// upper half-warp (the warp's second row) writes its second cell first (swap,
-// pa and pb exchanged), so that each store instruction writes odd and even
-// words: the two rows of the warp do not meet in one bank.  Every destination
-// of a tile pair lies inside the ring's margins: no test.
+// Ring writes of a source pair at tile position (px, py), px even: population
+// q goes to (px + c_x, py + c_y) and (px + 1 + c_x, py + c_y), where they are
+// inside the tile.  The in-x pair is one aligned 8-byte store; a shifted pair
+// is two 4-byte stores.
 template <int q, class E, class V>
-__device__ __forceinline__ void put_pair(const Ring<E>& R, int pos, int pa, int pb, V v, bool swap) {
+__device__ __forceinline__ void put_pair(const Ring<E>& R, int px, int py, V v) {
     constexpr int X = cx(q), Y = cy(q);
-    constexpr int d = X + Y * PITCH;
+    const int dy = py + Y;
+    if (dy < 0 || dy >= TY) return;
+    E* p = R.template at<q>(dy * TX + px + X);
     if constexpr (X == 0) {
-        st_pair(R.template at<q>(pos + d), v);
+        st_pair(p, v);
+    } else if constexpr (X > 0) {
+        p[0] = v.x;
+        if (px + 2 < TX) p[1] = v.y;
     } else {
-        *R.template at<q>(pa + d) = swap ? v.y : v.x;
-        *R.template at<q>(pb + d) = swap ? v.x : v.y;
+        if (px > 0) p[0] = v.x;
+        p[1] = v.y;
     }
 }
 template <int q, class E>
 __device__ __forceinline__ void put_one(const Ring<E>& R, int px, int py, E v) {
     const int dx = px + cx(q), dy = py + cy(q);
     if (dx < 0 || dx >= TX || dy < 0 || dy >= TY) return;
-    *R.template at<q>(rpos(dx, dy)) = v;
+    *R.template at<q>(dy * TX + dx) = v;
 }
 
 // halo-row positions build the populations that cross a y edge of the tile;
@@ -425,11 +418,6 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 4) home_step(HomePara
     // one aligned vector access for both cells: with nx even every plane, row
     // and moment plane starts at an even cell index, and the pair starts at an even x
     const bool vec = pair && e0 && e1 && c1 == c0 + 1 && (nx & 1) == 0;
-    // ring positions: the first cell's (gather, bounce-back slots), and the
-    // first and second cell's as the paired stores order them (see put_pair)
-    const int pos = rpos(px, py);
-    const bool swap = pair && (lane >> 4);
-    const int pa = swap ? pos + 1 : pos, pb = swap ? pos : pos + 1;
 
     V mreg[10];
 #pragma unroll
@@ -471,17 +459,12 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 4) home_step(HomePara
             if (role == ROLE_TILE) {
                 static_for<0, 19>([&](auto qi) {
                     constexpr int q = decltype(qi)::value;
-                    put_pair<q>(R, pos, pa, pb, fpost<q>(cf), swap);
+                    put_pair<q>(R, px, py, fpost<q>(cf));
                 });
             } else {
-                // halo rows: a population leaving the tile's rows lands in the
-                // margin row on the same side (written, never read)
                 for_qs<HOME_ROW_Q>([&](auto qi) {
                     constexpr int q = decltype(qi)::value;
-                    constexpr int Y = cy(q);
-                    const int dy = py + Y < -1 ? -1 : (py + Y > TY ? TY : py + Y);
-                    const int sh = (dy - py - Y) * PITCH;
-                    put_pair<q>(R, pos + sh, pa + sh, pb + sh, fpost<q>(cf), swap);
+                    put_pair<q>(R, px, py, fpost<q>(cf));
                 });
             }
         } else {
@@ -509,6 +492,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 8 ? 2 : 4) home_step(HomePara
     arrive(z0, u0);
     uint32_t fcur = freg;          // flags of the cells in the plane being gathered
     load(z0 + 1);
+    const int pos = py * TX + px;  // tile position of the first cell (owners)
 
     for (int z = z0; z < z1; ++z) {
         // 1. plane z+1 arrives (its moments were loaded one iteration ago); z+2 is requested

@@ -341,29 +341,19 @@ struct PlaneOffs {
 // ---------------------------------------------------------------------------
 // Odd step
 // ---------------------------------------------------------------------------
-// One odd-step cell: x of row `row` (= z*ny + y).
-template <class ST, bool MASK, int MODE, class IDX>
-__device__ __forceinline__ void odd_cell(const AAParams& p, const PlaneOffs<IDX>& po, IDX row, int x,
-                                         double (&acc)[NSTAT]) {
+// One fluid odd-step cell `id` = (x, y, z) with flag byte `fl`; nb gives its
+// neighbours' cell indices (nb.at(dx, dy, dz)).
+template <class ST, bool MASK, int MODE, class IDX, class NB>
+__device__ __forceinline__ void odd_core(const AAParams& p, const PlaneOffs<IDX>& po, IDX id, int x, int y, int z,
+                                         uint32_t fl, const NB& nb, double (&acc)[NSTAT]) {
     constexpr bool MACRO = MODE >= 1, STATS = MODE == 2;
     constexpr bool SH = kNarrow<ST>;    // narrow forms: compute in stored units
     using T = typename ST::T;
     using R = typename Real<ST>::type;
     T* __restrict__ f = static_cast<T*>(p.f);
-    const IDX N = (IDX)p.N;
     const int nx = p.nx, ny = p.ny, nz = p.nz;
     const R kin = R(1) + R(3) * p.u_in + R(3) * p.u_in * p.u_in;
     {
-        const int y = (int)(row % ny);
-        const int z = (int)(row / ny);
-        const IDX id = row * nx + x;
-        const uint32_t fl = MASK ? p.flags[id] : 0u;
-        if (MASK && (fl & F_SOLID)) {
-            if (MACRO) { p.rho[id] = 1.f; p.ux[id] = 0.f; p.uy[id] = 0.f; p.uz[id] = 0.f; }
-            return;
-        }
-        Nbr<IDX> nb;
-        nb.init(x, y, z, nx, ny, nz);
         uint32_t lk = 0u;
         if (MASK && (fl & F_SPECIAL)) lk = p.links[id];
         R c[19];
@@ -413,23 +403,94 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, const PlaneOffs<IDX>
     }
 }
 
-// Odd step: one cell per thread, rows of blockDim.x cells per block iteration.
+// A solid cell's odd step: frozen populations, rest-state macro fields.
+template <int MODE, class IDX>
+__device__ __forceinline__ void odd_solid(const AAParams& p, IDX id) {
+    if (MODE >= 1) { p.rho[id] = 1.f; p.ux[id] = 0.f; p.uy[id] = 0.f; p.uz[id] = 0.f; }
+}
+
+// One odd-step cell given by its row (= z*ny + y) and x (the batched step's form).
+template <class ST, bool MASK, int MODE, class IDX>
+__device__ __forceinline__ void odd_cell(const AAParams& p, const PlaneOffs<IDX>& po, IDX row, int x,
+                                         double (&acc)[NSTAT]) {
+    const int y = (int)(row % p.ny);
+    const int z = (int)(row / p.ny);
+    const IDX id = row * p.nx + x;
+    const uint32_t fl = MASK ? p.flags[id] : 0u;
+    if (MASK && (fl & F_SOLID)) {
+        odd_solid<MODE>(p, id);
+        return;
+    }
+    Nbr<IDX> nb;
+    nb.init(x, y, z, p.nx, p.ny, p.nz);
+    odd_core<ST, MASK, MODE, IDX>(p, po, id, x, y, z, fl, nb, acc);
+}
+
+// Neighbour addressing of a thread that marches along z at a fixed (x, y): the
+// three row offsets and x positions are formed once, and the three plane bases
+// (periodic in z) roll forward by one plane per step.
+template <class IDX>
+struct NbrZ {
+    IDX zb[3];     // [dz+1]: first cell of planes z-1, z, z+1
+    IDX yo[3];     // [dy+1]: first cell of rows y-1, y, y+1 inside a plane (periodic)
+    int xs[3];     // [dx+1]: x-1, x, x+1 (periodic)
+    __device__ __forceinline__ void init(int x, int y, int z, int nx, int ny, int nz) {
+        yo[0] = (IDX)(y == 0 ? ny - 1 : y - 1) * (IDX)nx;
+        yo[1] = (IDX)y * (IDX)nx;
+        yo[2] = (IDX)(y == ny - 1 ? 0 : y + 1) * (IDX)nx;
+        xs[0] = x == 0 ? nx - 1 : x - 1;
+        xs[1] = x;
+        xs[2] = x == nx - 1 ? 0 : x + 1;
+        const IDX plane = (IDX)nx * (IDX)ny;
+        zb[0] = (IDX)(z == 0 ? nz - 1 : z - 1) * plane;
+        zb[1] = (IDX)z * plane;
+        zb[2] = (IDX)(z == nz - 1 ? 0 : z + 1) * plane;
+    }
+    // from plane z to plane z + 1
+    __device__ __forceinline__ void advance(int z, int nz, IDX plane) {
+        zb[0] = zb[1];
+        zb[1] = zb[2];
+        zb[2] = z + 2 >= nz ? (IDX)(z + 2 - nz) * plane : zb[2] + plane;
+    }
+    __device__ __forceinline__ IDX at(int dx, int dy, int dz) const { return zb[dz + 1] + yo[dy + 1] + (IDX)xs[dx + 1]; }
+    __device__ __forceinline__ IDX id() const { return zb[1] + yo[1] + (IDX)xs[1]; }
+};
+
+// Odd step: a block owns blockDim.x cells of one row segment (one y) over a run
+// of p.zrun consecutive planes and marches along z, one cell per thread and
+// plane.  The grid holds every (segment, y, run) once (aa_odd_blocks), so the
+// hardware balances the runs over the SMs; the neighbour addressing costs a few
+// instructions per plane instead of a division and nine row products per cell.
 template <class ST, bool MASK, int MODE, class IDX>
 __global__ void __launch_bounds__(256, ST::kId == 3 ? 2 : (MASK ? 4 : 3)) aa_odd(AAParams p) {
     constexpr bool STATS = MODE == 2;
     const int bx = blockDim.x;
     const int segs = (p.nx + bx - 1) / bx;
-    const IDX row0 = (IDX)(p.first / p.nx);
-    const IDX total = (IDX)segs * (IDX)(p.cells / p.nx);
+    const IDX plane = (IDX)p.nx * (IDX)p.ny;
+    const int zlo = (int)(p.first / (int64_t)plane);
+    const int zhi = (int)((p.first + p.cells) / (int64_t)plane);
+    int b = (int)blockIdx.x;
+    const int seg = b % segs;
+    b /= segs;
+    const int y = b % p.ny;
+    const int z0 = zlo + (b / p.ny) * p.zrun;
+    const int z1 = min(zhi, z0 + p.zrun);
+    const int x = seg * bx + (int)threadIdx.x;
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-    PlaneOffs<IDX> po;
-    po.init((IDX)p.N);
-    for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
-        const IDX row = row0 + sg / segs;
-        const int x = (int)(sg - (sg / segs) * segs) * bx + threadIdx.x;
-        if (x < p.nx) odd_cell<ST, MASK, MODE, IDX>(p, po, row, x, acc);
+    if (x < p.nx) {
+        PlaneOffs<IDX> po;
+        po.init((IDX)p.N);
+        NbrZ<IDX> nb;
+        nb.init(x, y, z0, p.nx, p.ny, p.nz);
+        for (int z = z0; z < z1; ++z) {
+            const IDX id = nb.id();
+            const uint32_t fl = MASK ? p.flags[id] : 0u;
+            if (MASK && (fl & F_SOLID)) odd_solid<MODE>(p, id);
+            else odd_core<ST, MASK, MODE, IDX>(p, po, id, x, y, z, fl, nb, acc);
+            nb.advance(z, p.nz, plane);
+        }
     }
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }
@@ -462,12 +523,34 @@ __global__ void aa_materialize(AAParams p, int parity, float* __restrict__ out) 
     }
 }
 
+}  // namespace
+
+// Planes per block of the odd step: the longest run (at most 8) that still
+// leaves about eight waves of resident blocks, so the hardware's block
+// scheduling keeps the SMs evenly loaded to the end of the launch.
+int aa_odd_zrun(int nx, int ny, int64_t planes, bool mask, int storage, int threads) {
+    const int64_t segs = (nx + threads - 1) / threads;
+    const int bps = storage == 3 ? 2 : (mask ? 4 : 3);     // aa_odd's launch bounds
+    const int64_t target = (int64_t)num_sms() * bps * 8;
+    const int64_t run = segs * ny * planes / std::max<int64_t>(target, 1);
+    return (int)std::min<int64_t>(std::max<int64_t>(run, 1), 8);
+}
+
+int64_t aa_odd_blocks(int nx, int ny, int64_t planes, bool mask, int storage, int threads) {
+    const int64_t segs = (nx + threads - 1) / threads;
+    const int run = aa_odd_zrun(nx, ny, planes, mask, storage, threads);
+    return segs * ny * ((planes + run - 1) / run);
+}
+
+namespace {
+
 template <class ST, int MODE, class IDX>
 void launch_mode(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
     const bool mask = p.flags != nullptr;
-    // consecutive cells per thread: two in FP32 (8-byte accesses), four in F16/BF16 (8-byte
-    // accesses), one in FP64 (8-byte accesses)
-    constexpr int V = ST::kId == 0 ? 2 : (ST::kId == 3 ? 1 : 4);
+    // consecutive cells per thread: four in FP32 (16-byte accesses; two, with 8-byte accesses,
+    // when the launch also writes macro fields or statistics, which would spill at four), four
+    // in F16/BF16 (8-byte accesses), one in FP64 (8-byte accesses)
+    constexpr int V = ST::kId == 0 ? (MODE == 0 ? 4 : 2) : (ST::kId == 3 ? 1 : 4);
     if (parity == 0) {
         const int64_t span = p.first | p.cells;      // both must be multiples of the vector width
         if (V == 4 && span % 4 != 0 && span % 2 == 0) {
@@ -481,8 +564,13 @@ void launch_mode(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
             else aa_even<ST, false, 1, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
         }
     } else {
-        if (mask) aa_odd<ST, true, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
-        else aa_odd<ST, false, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+        const int64_t planes = p.cells / ((int64_t)p.nx * p.ny);
+        AAParams q = p;
+        q.zrun = aa_odd_zrun(p.nx, p.ny, planes, mask, ST::kId, cfg.threads);
+        const int64_t blocks = aa_odd_blocks(p.nx, p.ny, planes, mask, ST::kId, cfg.threads);
+        if (blocks <= 0) return;
+        if (mask) aa_odd<ST, true, MODE, IDX><<<(unsigned)blocks, cfg.threads, 0, s>>>(q);
+        else aa_odd<ST, false, MODE, IDX><<<(unsigned)blocks, cfg.threads, 0, s>>>(q);
     }
 }
 

@@ -32,6 +32,7 @@ struct AAParams {
     // ghost copies of the neighbouring slabs' boundary planes
     int64_t first, cells;
     uint32_t salt_base;      // F16/BF16 stochastic rounding: index of cell 0 in the whole grid
+    int zrun;                // odd step: planes per block (set by launch_aa_step)
 };
 
 // Parameters of one HOME step (moment-only, two buffers).
@@ -65,6 +66,10 @@ struct LaunchCfg {
 // AA steps.  parity 0: natural layout in (the even, purely local step);
 // parity 1: the odd step (gathers from and scatters to neighbours).
 cudaError_t launch_aa_step(const AAParams& p, int storage, int parity, LaunchCfg cfg, cudaStream_t s);
+// the odd step's grid: blocks of `threads` cells of one row, each over a run of
+// aa_odd_zrun planes; one statistics partial per block
+int aa_odd_zrun(int nx, int ny, int64_t planes, bool mask, int storage, int threads);
+int64_t aa_odd_blocks(int nx, int ny, int64_t planes, bool mask, int storage, int threads);
 // One step of many instances in one persistent launch (FP32 populations, the
 // instances' flag bytes required); units: {instance, first, count, -} with
 // first/count in two-cell vectors (parity 0) or cells (parity 1).  stats != 0 writes NSTAT sums per unit into partials.

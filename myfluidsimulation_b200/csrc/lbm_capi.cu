@@ -228,8 +228,8 @@ static int enqueue_steps(lbm_solver* s, int n) {
             CK(lbm::launch_aa_step(p, s->storage, s->parity, cfg, s->stream));
             if (st)
                 s->last_stat_blocks = s->parity == 0 ? cfg.blocks
-                                                     : (int)lbm::aa_odd_blocks(p.nx, p.ny, p.cells / ((int64_t)p.nx * p.ny),
-                                                                               p.flags != nullptr, s->storage, cfg.threads);
+                                                     : (int)lbm::aa_odd_grid(p.nx, p.ny, p.cells / ((int64_t)p.nx * p.ny),
+                                                                             p.flags != nullptr, s->storage, cfg);
             s->parity ^= 1;
         } else {
             lbm::HomeParams p = home_params(s, st);
@@ -383,8 +383,8 @@ int lbm_create(const lbm_domain* dom, const lbm_options* opts, lbm_solver** out)
         }
         s->home_zchunk = std::min(zc, dom->nz);
     }
-    // the odd step's grid is largest with a mask (most resident blocks, shortest runs)
-    const int64_t odd_blocks = lbm::aa_odd_blocks(dom->nx, dom->ny, dom->nz, true, o.storage, s->cfg_odd.threads);
+    // the z-marching odd step's grid (solvers without a mask)
+    const int64_t odd_blocks = lbm::aa_odd_blocks(dom->nx, dom->ny, dom->nz, false, o.storage, s->cfg_odd.threads);
     s->max_blocks = (int)std::max<int64_t>({s->cfg_even.blocks, s->cfg_odd.blocks, odd_blocks,
                                             lbm::home_num_blocks(dom->nx, dom->ny, dom->nz, s->home_zchunk), 1});
     auto dmalloc = [&](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess; };

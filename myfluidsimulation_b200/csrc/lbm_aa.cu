@@ -409,13 +409,11 @@ __device__ __forceinline__ void odd_solid(const AAParams& p, IDX id) {
     if (MODE >= 1) { p.rho[id] = 1.f; p.ux[id] = 0.f; p.uy[id] = 0.f; p.uz[id] = 0.f; }
 }
 
-// One odd-step cell given by its row (= z*ny + y) and x (the batched step's form).
+// One odd-step cell (x, y, z).
 template <class ST, bool MASK, int MODE, class IDX>
-__device__ __forceinline__ void odd_cell(const AAParams& p, const PlaneOffs<IDX>& po, IDX row, int x,
-                                         double (&acc)[NSTAT]) {
-    const int y = (int)(row % p.ny);
-    const int z = (int)(row / p.ny);
-    const IDX id = row * p.nx + x;
+__device__ __forceinline__ void odd_cell_at(const AAParams& p, const PlaneOffs<IDX>& po, int x, int y, int z,
+                                            double (&acc)[NSTAT]) {
+    const IDX id = ((IDX)z * (IDX)p.ny + (IDX)y) * (IDX)p.nx + (IDX)x;
     const uint32_t fl = MASK ? p.flags[id] : 0u;
     if (MASK && (fl & F_SOLID)) {
         odd_solid<MODE>(p, id);
@@ -424,6 +422,13 @@ __device__ __forceinline__ void odd_cell(const AAParams& p, const PlaneOffs<IDX>
     Nbr<IDX> nb;
     nb.init(x, y, z, p.nx, p.ny, p.nz);
     odd_core<ST, MASK, MODE, IDX>(p, po, id, x, y, z, fl, nb, acc);
+}
+
+// One odd-step cell given by its row (= z*ny + y) and x (the batched step's form).
+template <class ST, bool MASK, int MODE, class IDX>
+__device__ __forceinline__ void odd_cell(const AAParams& p, const PlaneOffs<IDX>& po, IDX row, int x,
+                                         double (&acc)[NSTAT]) {
+    odd_cell_at<ST, MASK, MODE, IDX>(p, po, x, (int)(row % p.ny), (int)(row / p.ny), acc);
 }
 
 // Neighbour addressing of a thread that marches along z at a fixed (x, y): the
@@ -495,29 +500,35 @@ __global__ void __launch_bounds__(256, ST::kId == 3 ? 2 : (MASK ? 4 : 3)) aa_odd
     if constexpr (STATS) block_reduce_stats(acc, p.partials);
 }
 
-// Odd step over rows, for grids with a solid mask: one cell per thread, rows of
-// blockDim.x cells per block iteration (grid-stride over the rows).  At the 64
-// registers of 4 blocks/SM that the mask's flag and link reads leave, the
-// z-marching form's rolling addresses measured more instructions per cell
-// (20.6 against 18.1 warp-instructions) and a slower step on the duct.
+// Odd step over rows, for grids with a solid mask: one cell per thread; a block
+// takes every gridDim.x-th row of its x segment (blockIdx.y), and steps the row's
+// (y, z) by a fixed stride instead of dividing per cell.  At the 64 registers
+// of 4 blocks/SM that the mask's flag and link reads leave, the z-marching
+// form's rolling addresses measured more instructions per cell (20.6 against
+// 17.6 warp-instructions) and a slower step on the duct.
 template <class ST, int MODE, class IDX>
 __global__ void __launch_bounds__(256, ST::kId == 3 ? 2 : 4) aa_odd_rows(AAParams p) {
     constexpr bool STATS = MODE == 2;
-    const int bx = blockDim.x;
-    const int segs = (p.nx + bx - 1) / bx;
-    const IDX row0 = (IDX)(p.first / p.nx);
-    const IDX total = (IDX)segs * (IDX)(p.cells / p.nx);
+    const int x = (int)blockIdx.y * (int)blockDim.x + (int)threadIdx.x;
+    const int rows = (int)(p.cells / p.nx);
+    const int z0 = (int)(p.first / ((int64_t)p.nx * p.ny));
+    const int S = (int)gridDim.x;
+    const int sy = S % p.ny, sz = S / p.ny;           // the stride in (y, z)
+    int y = (int)blockIdx.x % p.ny, z = z0 + (int)blockIdx.x / p.ny;
     double acc[NSTAT];
 #pragma unroll
     for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-    PlaneOffs<IDX> po;
-    po.init((IDX)p.N);
-    for (IDX sg = blockIdx.x; sg < total; sg += gridDim.x) {
-        const IDX row = row0 + sg / segs;
-        const int x = (int)(sg - (sg / segs) * segs) * bx + threadIdx.x;
-        if (x < p.nx) odd_cell<ST, true, MODE, IDX>(p, po, row, x, acc);
+    if (x < p.nx) {
+        PlaneOffs<IDX> po;
+        po.init((IDX)p.N);
+        for (int r = (int)blockIdx.x; r < rows; r += S) {
+            odd_cell_at<ST, true, MODE, IDX>(p, po, x, y, z, acc);
+            y += sy;
+            z += sz;
+            if (y >= p.ny) { y -= p.ny; ++z; }
+        }
     }
-    if constexpr (STATS) block_reduce_stats(acc, p.partials);
+    if constexpr (STATS) block_reduce_stats(acc, p.partials + (size_t)blockIdx.y * gridDim.x * NSTAT);
 }
 
 // The natural-layout populations f^n (the reference's d_f after n steps).
@@ -568,7 +579,9 @@ int64_t aa_odd_blocks(int nx, int ny, int64_t planes, bool mask, int storage, in
 }
 
 int64_t aa_odd_grid(int nx, int ny, int64_t planes, bool mask, int storage, LaunchCfg cfg) {
-    return mask ? (int64_t)cfg.blocks : aa_odd_blocks(nx, ny, planes, false, storage, cfg.threads);
+    if (!mask) return aa_odd_blocks(nx, ny, planes, false, storage, cfg.threads);
+    const int segs = (nx + cfg.threads - 1) / cfg.threads;
+    return (int64_t)std::max(1, cfg.blocks / segs) * segs;
 }
 
 namespace {
@@ -594,7 +607,9 @@ void launch_mode(const AAParams& p, int parity, LaunchCfg cfg, cudaStream_t s) {
         }
     } else {
         if (mask) {
-            aa_odd_rows<ST, MODE, IDX><<<cfg.blocks, cfg.threads, 0, s>>>(p);
+            const int segs = (p.nx + cfg.threads - 1) / cfg.threads;
+            const dim3 grid((unsigned)std::max(1, cfg.blocks / segs), (unsigned)segs);
+            aa_odd_rows<ST, MODE, IDX><<<grid, cfg.threads, 0, s>>>(p);
             return;
         }
         const int64_t planes = p.cells / ((int64_t)p.nx * p.ny);

@@ -70,8 +70,9 @@ cudaError_t launch_aa_step(const AAParams& p, int storage, int parity, LaunchCfg
 // aa_odd_zrun planes; one statistics partial per block
 int aa_odd_zrun(int nx, int ny, int64_t planes, bool mask, int storage, int threads);
 int64_t aa_odd_blocks(int nx, int ny, int64_t planes, bool mask, int storage, int threads);
-// blocks of one odd-step launch: the z-marching grid without a mask, cfg.blocks
-// (rows, grid-stride) with one
+// blocks of one odd-step launch: the z-marching grid without a mask; with one,
+// cfg.blocks rounded down to a multiple of the row segments (a 2-D grid of
+// rows x segments)
 int64_t aa_odd_grid(int nx, int ny, int64_t planes, bool mask, int storage, LaunchCfg cfg);
 // One step of many instances in one persistent launch (FP32 populations, the
 // instances' flag bytes required); units: {instance, first, count, -} with

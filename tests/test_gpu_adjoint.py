@@ -102,6 +102,45 @@ def test_adjoint_matches_central_differences(gpu):
     print(f"central differences: worst relative difference {worst:.3e}")
 
 
+def test_full_case_matches_central_differences(gpu):
+    """The adjoint case at full size: duct 128x64x64, tau 0.6, sphere r = 10 at
+    (32,32,32), 500 steps, drag averaged over steps 400-500, checkpoints every
+    50 steps; inlet profile 0.04 + 0.005 N(0,1) smoothed by a 5x5 box filter and
+    initial velocity 0.04 + 1e-3 N(0,1).  Along 32 random unit directions in
+    control space, the FP64 and the FP32 adjoint gradients against central
+    differences of the FP64 objective (eps 1e-3): relative 1e-6 (FP64) and 1e-4
+    (FP32, the stated bound)."""
+    nx, ny, nz = 128, 64, 64
+    prob = DuctProblem(nx, ny, nz, 0.6, duct(nx, ny, nz, 10.0, (32, 32, 32)), n_steps=500, window=(400, 500),
+                       checkpoint_every=50)
+    import torch
+    gen = torch.Generator().manual_seed(4)          # the draws of `bench.py --study adjoint`
+    raw = (0.04 + 0.005 * torch.randn((nz + 4, ny + 4), generator=gen, dtype=torch.float64)).numpy()
+    k = np.ones(5) / 5
+    ui = np.apply_along_axis(lambda r: np.convolve(r, k, "valid"), 1, raw)
+    ui = np.apply_along_axis(lambda c: np.convolve(c, k, "valid"), 0, ui)
+    u0 = 1e-3 * torch.randn((3, nz, ny, nx), generator=gen, dtype=torch.float64).numpy()
+    u0[0] += 0.04
+    _, gi64, gu64 = objective(prob, ui, u0, "f64", grad=True)
+    _, gi32, gu32 = objective(prob, ui, u0, "f32", grad=True)
+    rng = np.random.default_rng(2026)
+    eps = 1e-3
+    worst64 = worst32 = 0.0
+    for _ in range(32):
+        di = rng.standard_normal(ui.shape)
+        du = rng.standard_normal(u0.shape)
+        scale = 1.0 / np.sqrt((di ** 2).sum() + (du ** 2).sum())
+        di *= scale
+        du *= scale
+        fd = (objective(prob, ui + eps * di, u0 + eps * du, "f64") -
+              objective(prob, ui - eps * di, u0 - eps * du, "f64")) / (2 * eps)
+        worst64 = max(worst64, abs(float((gi64 * di).sum() + (gu64 * du).sum()) - fd) / abs(fd))
+        worst32 = max(worst32, abs(float((gi32 * di).sum() + (gu32 * du).sum()) - fd) / abs(fd))
+    print(f"full case: worst relative difference FP64 {worst64:.3e}, FP32 {worst32:.3e}")
+    assert worst64 < 1e-6
+    assert worst32 < 1e-4
+
+
 def test_objective_matches_the_product_forward(gpu):
     """With a uniform inlet the adjoint's forward model is the AA duct step of
     lbm_step: the windowed drag agrees within FP32 rounding."""

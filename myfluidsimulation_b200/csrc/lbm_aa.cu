@@ -668,7 +668,9 @@ __device__ __forceinline__ void block_reduce_into(double (&acc)[NSTAT], double* 
     __syncthreads();
 }
 
-template <class ST, int MODE>
+// even units count vectors of VEC cells: two in FP32, four in F16/BF16 (the
+// single-solver step's vectors, so the stochastic rounding draws the same bits)
+template <class ST, int MODE, int VEC>
 __global__ void __launch_bounds__(256, 2) aa_batch_even(const AAParams* __restrict__ inst, const int4* __restrict__ units,
                                                      int nunits, double* __restrict__ partials) {
     constexpr bool STATS = MODE == 2;
@@ -682,7 +684,7 @@ __global__ void __launch_bounds__(256, 2) aa_batch_even(const AAParams* __restri
 #pragma unroll
         for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
         for (int v = w.y + threadIdx.x; v < w.y + w.z; v += blockDim.x)
-            even_unit<ST, true, 2, MODE, uint32_t>(p, (uint32_t)v, acc);
+            even_unit<ST, true, VEC, MODE, uint32_t>(p, (uint32_t)v, acc);
         if constexpr (STATS) block_reduce_into(acc, partials + (size_t)u * NSTAT);
     }
 }
@@ -728,16 +730,27 @@ __global__ void batch_finalize(const double* __restrict__ partials, const int* _
 
 }  // namespace
 
+template <class ST>
+void launch_batch_typed(const AAParams* d_inst, const int4* d_units, int nunits, int parity, int stats, int blocks,
+                        int threads, double* partials, cudaStream_t s) {
+    constexpr int V = ST::kId == 0 ? 2 : 4;
+    if (parity == 0) {
+        if (stats) aa_batch_even<ST, 2, V><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+        else aa_batch_even<ST, 0, V><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+    } else {
+        if (stats) aa_batch_odd<ST, 2><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+        else aa_batch_odd<ST, 0><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+    }
+}
+
 cudaError_t launch_aa_batch(const AAParams* d_inst, const int4* d_units, int nunits, int parity, int stats,
                             int storage, int blocks, int threads, double* partials, cudaStream_t s) {
-    if (storage != 0) return cudaErrorInvalidValue;   // the batch runs FP32 populations
     if (nunits <= 0) return cudaSuccess;
-    if (parity == 0) {
-        if (stats) aa_batch_even<StoreF32, 2><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
-        else aa_batch_even<StoreF32, 0><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
-    } else {
-        if (stats) aa_batch_odd<StoreF32, 2><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
-        else aa_batch_odd<StoreF32, 0><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+    switch (storage) {
+        case 0: launch_batch_typed<StoreF32>(d_inst, d_units, nunits, parity, stats, blocks, threads, partials, s); break;
+        case 1: launch_batch_typed<StoreF16>(d_inst, d_units, nunits, parity, stats, blocks, threads, partials, s); break;
+        case 2: launch_batch_typed<StoreBF16>(d_inst, d_units, nunits, parity, stats, blocks, threads, partials, s); break;
+        default: return cudaErrorInvalidValue;   // the batch runs FP32, F16 or BF16 populations
     }
     return cudaGetLastError();
 }

@@ -1131,6 +1131,8 @@ struct lbm_batch {
     int* d_first[2] = {nullptr, nullptr};
     int nunits[2] = {0, 0};
     int units_threads = 0, units_even = 0, units_odd = 0;   // shape the unit lists were built for
+    int storage = LBM_STORE_F32;   // of every instance
+    int vec = 2;                   // cells per vector of the even step: 2 (FP32), 4 (F16/BF16)
     double* partials = nullptr;
     size_t partials_cap = 0;
     double* d_stats = nullptr;
@@ -1177,7 +1179,7 @@ int batch_build_units(lbm_batch* b) {
         for (size_t i = 0; i < b->inst.size(); ++i) {
             const lbm_solver* s = b->inst[i];
             first.push_back((int)u.size());
-            const int64_t total = par == 0 ? s->N / 2 : s->N;
+            const int64_t total = par == 0 ? s->N / b->vec : s->N;
             const int step = par == 0 ? E : O * T;
             for (int64_t f = 0; f < total; f += step)
                 u.push_back(make_int4((int)i, (int)f, (int)std::min<int64_t>(step, total - f), 0));
@@ -1211,7 +1213,7 @@ int batch_enqueue(lbm_batch* b, int n) {
         const bool st = b->stats_on && i == n - 1;
         const int par = b->parity;
         const int blocks = std::max(1, std::min(blocks_cap, b->nunits[par]));
-        CK(lbm::launch_aa_batch(b->d_params, b->d_units[par], b->nunits[par], par, st, 0, blocks, b->tune.threads,
+        CK(lbm::launch_aa_batch(b->d_params, b->d_units[par], b->nunits[par], par, st, b->storage, blocks, b->tune.threads,
                                 b->partials, b->stream));
         if (st) CK(lbm::launch_batch_finalize(b->partials, b->d_first[par], (int)b->inst.size(), b->d_stats, b->stream));
         b->parity ^= 1;
@@ -1236,16 +1238,19 @@ int lbm_batch_create(lbm_solver* const* solvers, int32_t n, void* stream, lbm_ba
     for (int i = 0; i < n; ++i) {
         const lbm_solver* s = solvers[i];
         if (!s) { set_error("lbm_batch_create: null solver"); return LBM_ERR_INVALID; }
-        if (!is_aa(s) || is_ref_push(s) || s->storage != LBM_STORE_F32) {
-            set_error("lbm_batch_create: instances must be Legacy/Hybrid, FP32, halfway bounce-back");
+        if (!is_aa(s) || is_ref_push(s) || s->storage == LBM_STORE_F64 || s->storage != solvers[0]->storage) {
+            set_error("lbm_batch_create: instances must be Legacy/Hybrid, halfway bounce-back, all in one of "
+                      "FP32, F16 or BF16 storage");
             return LBM_ERR_UNSUPPORTED;
         }
         if (s->zghost) {
             set_error("lbm_batch_create: z-slab solvers (ghost planes) cannot be batched");
             return LBM_ERR_UNSUPPORTED;
         }
-        if (s->N % 2 != 0 || (uint64_t)s->N * 19u >= (1ull << 32)) {
-            set_error("lbm_batch_create: instance cell counts must be even and below 2^32/19");
+        const int vec = s->storage == LBM_STORE_F32 ? 2 : 4;
+        if (s->N % vec != 0 || (uint64_t)s->N * 19u >= (1ull << 32)) {
+            set_error("lbm_batch_create: instance cell counts must be multiples of 2 (FP32) or 4 (F16/BF16) "
+                      "and below 2^32/19");
             return LBM_ERR_SIZE;
         }
         if (s->parity != solvers[0]->parity) {
@@ -1255,6 +1260,8 @@ int lbm_batch_create(lbm_solver* const* solvers, int32_t n, void* stream, lbm_ba
     }
     lbm_batch* b = new lbm_batch();
     b->inst.assign(solvers, solvers + n);
+    b->storage = solvers[0]->storage;
+    b->vec = b->storage == LBM_STORE_F32 ? 2 : 4;
     b->parity = solvers[0]->parity;
     if (stream) b->stream = static_cast<cudaStream_t>(stream);
     else {

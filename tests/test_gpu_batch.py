@@ -9,7 +9,7 @@ import pytest
 from myfluidsimulation_b200 import workloads as W
 from myfluidsimulation_b200._lib import LBMError
 from myfluidsimulation_b200.solvers import (BC_DUCT, BC_PERIODIC, METHOD_HOME, METHOD_HYBRID, METHOD_LEGACY,
-                                            STORE_F16, Batch, Solver)
+                                            STORE_BF16, STORE_F16, STORE_F32, STORE_F64, Batch, Solver)
 
 pytestmark = pytest.mark.gpu
 
@@ -24,7 +24,7 @@ SPECS = [
 ]
 
 
-def make(spec, seed):
+def make(spec, seed, storage=STORE_F32):
     dims, tau, method, bc, b0 = spec
     nx, ny, nz = dims
     rng = np.random.default_rng(seed)
@@ -34,7 +34,7 @@ def make(spec, seed):
     if bc == BC_DUCT:
         mask = W.duct_mask(nx, ny, nz, mask)
     s = Solver(nx, ny, nz, tau, (1e-6, 0, 0) if bc == BC_PERIODIC else (0, 0, 0), method=method, bc=bc,
-               inlet_u=0.04)
+               inlet_u=0.04, storage=storage)
     s.set_solid_mask(mask)
     if method == METHOD_HYBRID:
         s.build_band(b0)
@@ -44,10 +44,10 @@ def make(spec, seed):
     return s
 
 
-def run_single(steps_list, stats=False):
+def run_single(steps_list, stats=False, storage=STORE_F32):
     out = []
     for i, spec in enumerate(SPECS):
-        s = make(spec, i)
+        s = make(spec, i, storage)
         s.enable_stats(stats)
         for n in steps_list:
             s.step(n)
@@ -67,6 +67,26 @@ def test_batch_bit_identical_to_single(gpu, steps_list):
     b.synchronize()
     for (st, _), s in zip(ref, solvers):
         np.testing.assert_array_equal(s.state(), st)
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+@pytest.mark.parametrize("storage", [STORE_F16, STORE_BF16])
+def test_narrow_batch_bit_identical_to_single(gpu, storage):
+    """F16/BF16 instances: the batch's even step takes the single solver's
+    four-cell vectors, and the stochastic rounding draws its bits by cell index,
+    so batched states equal the single-instance ones bit for bit."""
+    ref = run_single([3, 20, 1], stats=True, storage=storage)
+    solvers = [make(spec, i, storage) for i, spec in enumerate(SPECS)]
+    b = Batch(solvers)
+    b.enable_stats(True)
+    for n in (3, 20, 1):
+        b.step(n)
+    st = b.stats()
+    for i, ((state, sref), s) in enumerate(zip(ref, solvers)):
+        np.testing.assert_array_equal(s.state(), state)
+        assert st[i, 0] == pytest.approx(sref["mass"], rel=1e-11), i
     b.close()
     for s in solvers:
         s.close()
@@ -121,12 +141,19 @@ def test_batch_rejects_unsupported_instances(gpu):
     a = Solver(16, 16, 16, 0.6, method=METHOD_HOME)
     c = Solver(16, 16, 16, 0.6, method=METHOD_LEGACY, storage=STORE_F16)
     d = Solver(16, 16, 16, 0.6, method=METHOD_LEGACY)
-    for bad in ([a], [c], [d, a]):
+    f = Solver(16, 16, 16, 0.6, method=METHOD_LEGACY, storage=STORE_F64)
+    g = Solver(18, 15, 15, 0.6, method=METHOD_LEGACY, storage=STORE_BF16)   # 4050 cells: not a multiple of 4
+    h = Solver(18, 15, 15, 0.6, method=METHOD_LEGACY)                        # even: fine in FP32
+    for bad in ([a], [d, a], [d, c], [f], [g]):
         with pytest.raises(LBMError):
             Batch(bad)
+    for ok in ([c], [h]):
+        Batch(ok).close()
+    for s in (c, f, g, h):
+        s.close()
     d.step(1)
     e = Solver(16, 16, 16, 0.6, method=METHOD_LEGACY)
     with pytest.raises(LBMError):
         Batch([d, e])               # different parities
-    for s in (a, c, d, e):
+    for s in (a, d, e):
         s.close()

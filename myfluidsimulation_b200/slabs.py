@@ -132,6 +132,7 @@ class SlabSet:
         self.stream = stream if stream is not None else torch.cuda.current_stream().cuda_stream
         self.slabs = []
         self._plan = None
+        self._stats, self._macro = False, True
         self.home = method == METHOD_HOME
         for z0, z1 in self.bounds:
             s = Solver(nx, ny, z1 - z0 + 2, tau, force, method=method, storage=storage, bc=bc, inlet_u=inlet_u,
@@ -163,6 +164,7 @@ class SlabSet:
                                                                      z0, z1) for a in (rho, ux, uy, uz)])
 
     def enable_stats(self, on=True):
+        self._stats = bool(on)
         for s in self.slabs:
             s.enable_stats(on)
 
@@ -171,8 +173,17 @@ class SlabSet:
             s.set_shear_omega(omega_s)
 
     def set_macro_output(self, on=True):
+        self._macro = bool(on)
         for s in self.slabs:
             s.set_macro_output(on)
+
+    def _outputs(self, on):
+        """Statistics and macro fields as set (on) or off: the slabs step one
+        substep per call, so n steps leave them off for all but the last, as
+        lbm_step(n) does."""
+        for s in self.slabs:
+            s.enable_stats(self._stats and on)
+            s.set_macro_output(self._macro and on)
 
     def _ensure_plan(self):
         # every face in one launch per phase (lbm_zslab_plan_*), built after the mask and band
@@ -211,7 +222,12 @@ class SlabSet:
         return g
 
     def step(self, n: int = 1):
-        for _ in range(n):
+        quiet = n > 1 and (self._stats or self._macro)
+        if quiet:
+            self._outputs(False)
+        for k in range(n):
+            if quiet and k == n - 1:
+                self._outputs(True)
             ex = self.home or _parity(self.slabs[0]) == 1
             if ex:
                 self._exchange(0)
@@ -286,6 +302,8 @@ class DistSlab:
         self.views = {}
         self._home_views = {}
         self._pending = []          # phase-1 works of an overlapped odd step, merged before the next use
+        self._plan = None           # one rank: the self-exchange plan (lbm_zslab_plan_*)
+        self._stats, self._macro = False, True
         if not self.home:
             for name, pl in planes.items():
                 for cz in (+1, -1):
@@ -358,9 +376,25 @@ class DistSlab:
             self._planes(1, 2, False)
             self._planes(L - 2, L - 1, True)
 
+    def _drop_plan(self):
+        if self._plan:
+            check(lib().lbm_zslab_plan_destroy(self._plan))
+            self._plan = None
+
     def _exchange(self, phase):
         if self.world == 1:
-            check(lib().lbm_zslab_exchange(self.solver._h, self.solver._h, phase, C.c_void_p(self.solver.stream)))
+            # one self-neighbouring slab: both faces of a phase in one launch of the
+            # exchange plan (HOME's moment planes move per face, between buffers that swap)
+            if self.home:
+                check(lib().lbm_zslab_exchange(self.solver._h, self.solver._h, phase,
+                                               C.c_void_p(self.solver.stream)))
+                return
+            if self._plan is None:
+                hs = (C.c_void_p * 1)(self.solver._h.value)
+                p = C.c_void_p()
+                check(lib().lbm_zslab_plan_create(hs, 1, C.byref(p)))
+                self._plan = p
+            check(lib().lbm_zslab_plan_exchange(self._plan, phase, C.c_void_p(self.solver.stream)))
             return
         if self.home:
             if phase == 0:
@@ -374,9 +408,11 @@ class DistSlab:
 
     def set_solid_mask(self, mask):
         self.solver.set_solid_mask(with_ghosts(np.asarray(mask, np.uint8).reshape(self.shape), self.z0, self.z1))
+        self._drop_plan()           # the plan holds the flag and link planes of the mask it was built for
 
     def set_legacy_mapping(self, band):
         self.solver.set_legacy_mapping(with_ghosts(np.asarray(band, np.uint8).reshape(self.shape), self.z0, self.z1))
+        self._drop_plan()
 
     def reinit_from_host(self, rho=None, ux=None, uy=None, uz=None):
         self.solver.reinit_from_host(*[None if a is None else with_ghosts(
@@ -388,10 +424,16 @@ class DistSlab:
         step but the last, which runs whole, so that its statistics and macro
         fields come out as from lbm_step."""
         can = overlap and not self.home and self.world > 1 and self.planes["ghost_hi"] - 1 >= 3
+        # one substep per call: statistics and macro fields only on the last, as lbm_step(n)
+        quiet = n > 1 and (self._stats or self._macro)
+        if quiet:
+            self._outputs(False)
         for k in range(n):
             if can and k < n - 1:
                 self._step_overlapped()
                 continue
+            if quiet and k == n - 1:
+                self._outputs(True)
             self._flush()
             ex = self.home or _parity(self.solver) == 1
             if ex:
@@ -404,7 +446,16 @@ class DistSlab:
         self.solver.set_shear_omega(omega_s)
 
     def enable_stats(self, on=True):
+        self._stats = bool(on)
         self.solver.enable_stats(on)
+
+    def set_macro_output(self, on=True):
+        self._macro = bool(on)
+        self.solver.set_macro_output(on)
+
+    def _outputs(self, on):
+        self.solver.enable_stats(self._stats and on)
+        self.solver.set_macro_output(self._macro and on)
 
     def synchronize(self):
         self._flush()
@@ -430,4 +481,5 @@ class DistSlab:
 
     def close(self):
         self._flush()
+        self._drop_plan()
         self.solver.close()

@@ -182,7 +182,8 @@ class _FakeDist:
         return [self._Work() for _ in ops]
 
 
-@pytest.mark.parametrize("world,method,overlap", [(2, METHOD_LEGACY, False), (3, METHOD_HYBRID, False),
+@pytest.mark.parametrize("world,method,overlap", [(1, METHOD_LEGACY, False), (1, METHOD_HOME, False),
+                                                  (2, METHOD_LEGACY, False), (3, METHOD_HYBRID, False),
                                                   (3, METHOD_HOME, False), (2, METHOD_LEGACY, True),
                                                   (3, METHOD_HYBRID, True)])
 def test_dist_slabs_equal_single_grid(gpu, oracle, world, method, overlap):

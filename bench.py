@@ -1065,8 +1065,9 @@ def decomp_run(args, torch, dist, rank, world):
                          "transport": "NCCL point to point, overlapped with interior planes" if world > 1 else
                                       "self-exchange (one slab, device copies)"},
             # per step pair: the even and odd kernels (3 parts each when overlapped) and the
-            # 10 merge kernels of phase 1; plus the statistics' final pass per bench step
-            "gpu_launches": args.steps * ((DRAG_EVERY // 2) * (16 if world > 1 else 12) + 1),
+            # 10 merge kernels of phase 1 (one rank: the two steps and one exchange-plan launch
+            # per phase); plus the statistics' final pass per bench step
+            "gpu_launches": args.steps * ((DRAG_EVERY // 2) * (16 if world > 1 else 4) + 1),
             "stats": {"mass": stats["mass"], "drag": [stats["drag_x"], stats["drag_y"], stats["drag_z"]]},
             "clocks": clk.summary()}))
 

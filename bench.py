@@ -231,12 +231,15 @@ def kernel_split(s, method, torch, launches=40):
     return {names[0]: round(2 * mean_us * a / (a + b), 2), names[1]: round(2 * mean_us * b / (a + b), 2)}
 
 
-def run_method(method, workload, mask, args, torch):
+def run_method(method, workload, mask, args, torch, dist=None):
     st = torch.cuda.current_stream()
     s, nb = make_solver(method, workload, mask, st.cuda_stream)
     for _ in range(args.warmup):
         s.step(DRAG_EVERY)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+        torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(st)
@@ -244,6 +247,8 @@ def run_method(method, workload, mask, args, torch):
         s.step(DRAG_EVERY)
     e1.record(st)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     ms = e0.elapsed_time(e1)
     st_ = s.stats()
     res = {"ms_total": ms, "launches": args.steps * (DRAG_EVERY + 1), "band_cells": nb,
@@ -252,7 +257,7 @@ def run_method(method, workload, mask, args, torch):
     return s, res
 
 
-def e2e_run(method, workload, mask, args, torch):
+def e2e_run(method, workload, mask, args, torch, dist=None):
     """Through the public C-ABI with host buffers: every step uploads the macro
     fields from pinned host memory, reinitialises from them, runs one drag
     interval and reads the macro fields and the statistics back.  The copies of
@@ -293,6 +298,9 @@ def e2e_run(method, workload, mask, args, torch):
 
     run(max(2, args.warmup // 2))
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+        torch.cuda.synchronize()
     t0 = time.perf_counter()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -1192,7 +1200,7 @@ def main():
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
-        s, r = run_method(mth, wl, mask, args, torch)
+        s, r = run_method(mth, wl, mask, args, torch, dist)
         ms = torch.tensor([r["ms_total"]], device="cuda")
         if dist:
             dist.all_reduce(ms, op=dist.ReduceOp.MAX)
@@ -1225,7 +1233,7 @@ def main():
     clocks = clk.summary()
     # end to end through the C-ABI with host buffers (headline run)
     hm, hw = keys[head]
-    e2e_ms, e2e_wall, h2d, d2h = e2e_run(hm, hw, mask, args, torch)
+    e2e_ms, e2e_wall, h2d, d2h = e2e_run(hm, hw, mask, args, torch, dist)
     e2e_t = torch.tensor([e2e_ms], device="cuda")
     if dist:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)

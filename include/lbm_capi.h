@@ -239,8 +239,7 @@ int lbm_macro_stats_static(const float* d_rho, const float* d_ux, const float* d
 /* ---- batched instances ------------------------------------------------- */
 
 /* Many independent Legacy/Hybrid solvers (halfway bounce-back; all in FP32,
- * all in F16 or all in BF16 storage; cell counts multiples of 2 in FP32 and of
- * 4 in F16/BF16; any sizes, rates, bands and boundaries)
+ * all in F16 or all in BF16 storage; any sizes, rates, bands and boundaries)
  * advanced together: every substep is ONE persistent launch over all of them,
  * and a multi-step lbm_batch_step is replayed from a captured CUDA graph.  No
  * reference counterpart: the reference runs one solver per process and times
@@ -250,7 +249,8 @@ typedef struct lbm_batch lbm_batch;
 typedef struct lbm_batch_tuning {
     int32_t threads;         /* threads per block (128 or 256) */
     int32_t blocks_per_sm;   /* persistent blocks per SM */
-    int32_t even_unit;       /* vectors (2 cells in FP32, 4 in F16/BF16) per work unit of the local step */
+    int32_t even_unit;       /* vectors (of the width each instance's own step takes: 1, 2 or 4 cells)
+                                per work unit of the local step */
     int32_t odd_unit;        /* blocks of `threads` cells per unit of the neighbour step */
     float us_per_step;       /* measured by lbm_batch_tune: mean of one even + one odd launch / 2 */
 } lbm_batch_tuning;

@@ -256,7 +256,11 @@ __device__ __forceinline__ void even_unit(const AAParams& p, IDX v, double (&acc
                                  p.nx, p.ny, p.nz, p.duct);
                 }
             }
-            const int x = x0 + l;
+            // a vector may run past the end of its row when nx is not a multiple of
+            // VEC (l conditional subtractions cover any nx >= 1)
+            int x = x0 + l;
+#pragma unroll
+            for (int k = 0; k < l; ++k) x = x >= p.nx ? x - p.nx : x;
             const bool at_in = p.duct && x == 0, at_out = p.duct && x == p.nx - 1;
 #pragma unroll
             for (int q = 0; q < 19; ++q) {
@@ -668,9 +672,10 @@ __device__ __forceinline__ void block_reduce_into(double (&acc)[NSTAT], double* 
     __syncthreads();
 }
 
-// even units count vectors of VEC cells: two in FP32, four in F16/BF16 (the
-// single-solver step's vectors, so the stochastic rounding draws the same bits)
-template <class ST, int MODE, int VEC>
+// Even units count vectors of w.w cells: the single solver's vector width for
+// the instance's cell count (F16/BF16: 4, 2 or 1; FP32: 2 or 1), so the
+// stochastic rounding draws the same bits as stepping the instance alone.
+template <class ST, int MODE>
 __global__ void __launch_bounds__(256, 2) aa_batch_even(const AAParams* __restrict__ inst, const int4* __restrict__ units,
                                                      int nunits, double* __restrict__ partials) {
     constexpr bool STATS = MODE == 2;
@@ -683,8 +688,15 @@ __global__ void __launch_bounds__(256, 2) aa_batch_even(const AAParams* __restri
         double acc[NSTAT];
 #pragma unroll
         for (int k = 0; k < NSTAT; ++k) acc[k] = 0.0;
-        for (int v = w.y + threadIdx.x; v < w.y + w.z; v += blockDim.x)
-            even_unit<ST, true, VEC, MODE, uint32_t>(p, (uint32_t)v, acc);
+        for (int v = w.y + threadIdx.x; v < w.y + w.z; v += blockDim.x) {
+            if (kNarrow<ST> && w.w == 4) {
+                if constexpr (kNarrow<ST>) even_unit<ST, true, 4, MODE, uint32_t>(p, (uint32_t)v, acc);
+            } else if (w.w == 2) {
+                even_unit<ST, true, 2, MODE, uint32_t>(p, (uint32_t)v, acc);
+            } else {
+                even_unit<ST, true, 1, MODE, uint32_t>(p, (uint32_t)v, acc);
+            }
+        }
         if constexpr (STATS) block_reduce_into(acc, partials + (size_t)u * NSTAT);
     }
 }
@@ -733,10 +745,9 @@ __global__ void batch_finalize(const double* __restrict__ partials, const int* _
 template <class ST>
 void launch_batch_typed(const AAParams* d_inst, const int4* d_units, int nunits, int parity, int stats, int blocks,
                         int threads, double* partials, cudaStream_t s) {
-    constexpr int V = ST::kId == 0 ? 2 : 4;
     if (parity == 0) {
-        if (stats) aa_batch_even<ST, 2, V><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
-        else aa_batch_even<ST, 0, V><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+        if (stats) aa_batch_even<ST, 2><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
+        else aa_batch_even<ST, 0><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
     } else {
         if (stats) aa_batch_odd<ST, 2><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);
         else aa_batch_odd<ST, 0><<<blocks, threads, 0, s>>>(d_inst, d_units, nunits, partials);

@@ -1132,7 +1132,6 @@ struct lbm_batch {
     int nunits[2] = {0, 0};
     int units_threads = 0, units_even = 0, units_odd = 0;   // shape the unit lists were built for
     int storage = LBM_STORE_F32;   // of every instance
-    int vec = 2;                   // cells per vector of the even step: 2 (FP32), 4 (F16/BF16)
     double* partials = nullptr;
     size_t partials_cap = 0;
     double* d_stats = nullptr;
@@ -1169,6 +1168,14 @@ int batch_upload_params(lbm_batch* b) {
     return LBM_OK;
 }
 
+// cells per vector of an instance's batched even step: the width its own step
+// takes for its cell count (F16/BF16: 4, 2 or 1; FP32, whose results do not
+// depend on it: 2 or 1)
+int batch_vec(const lbm_solver* s) {
+    if (s->storage == LBM_STORE_F32) return s->N % 2 == 0 ? 2 : 1;
+    return s->N % 4 == 0 ? 4 : (s->N % 2 == 0 ? 2 : 1);
+}
+
 // unit lists of both parities for the current launch shape
 int batch_build_units(lbm_batch* b) {
     const int T = b->tune.threads, E = b->tune.even_unit, O = b->tune.odd_unit;
@@ -1179,10 +1186,12 @@ int batch_build_units(lbm_batch* b) {
         for (size_t i = 0; i < b->inst.size(); ++i) {
             const lbm_solver* s = b->inst[i];
             first.push_back((int)u.size());
-            const int64_t total = par == 0 ? s->N / b->vec : s->N;
+            // even step: vectors of the width the instance's own step would use
+            const int vec = batch_vec(s);
+            const int64_t total = par == 0 ? s->N / vec : s->N;
             const int step = par == 0 ? E : O * T;
             for (int64_t f = 0; f < total; f += step)
-                u.push_back(make_int4((int)i, (int)f, (int)std::min<int64_t>(step, total - f), 0));
+                u.push_back(make_int4((int)i, (int)f, (int)std::min<int64_t>(step, total - f), par == 0 ? vec : 0));
         }
         first.push_back((int)u.size());
         cudaFree(b->d_units[par]);
@@ -1247,10 +1256,8 @@ int lbm_batch_create(lbm_solver* const* solvers, int32_t n, void* stream, lbm_ba
             set_error("lbm_batch_create: z-slab solvers (ghost planes) cannot be batched");
             return LBM_ERR_UNSUPPORTED;
         }
-        const int vec = s->storage == LBM_STORE_F32 ? 2 : 4;
-        if (s->N % vec != 0 || (uint64_t)s->N * 19u >= (1ull << 32)) {
-            set_error("lbm_batch_create: instance cell counts must be multiples of 2 (FP32) or 4 (F16/BF16) "
-                      "and below 2^32/19");
+        if ((uint64_t)s->N * 19u >= (1ull << 32)) {
+            set_error("lbm_batch_create: instance cell counts must be below 2^32/19");
             return LBM_ERR_SIZE;
         }
         if (s->parity != solvers[0]->parity) {
@@ -1261,7 +1268,6 @@ int lbm_batch_create(lbm_solver* const* solvers, int32_t n, void* stream, lbm_ba
     lbm_batch* b = new lbm_batch();
     b->inst.assign(solvers, solvers + n);
     b->storage = solvers[0]->storage;
-    b->vec = b->storage == LBM_STORE_F32 ? 2 : 4;
     b->parity = solvers[0]->parity;
     if (stream) b->stream = static_cast<cudaStream_t>(stream);
     else {

@@ -44,9 +44,17 @@ def make(spec, seed, storage=STORE_F32):
     return s
 
 
-def run_single(steps_list, stats=False, storage=STORE_F32):
+# cell counts that are odd (1575), even but not a multiple of 4 (4050) and a multiple of 4 (2700)
+SPECS_ODD = [
+    ((25, 9, 7), 0.6, METHOD_LEGACY, BC_PERIODIC, 0),
+    ((18, 15, 15), 0.57, METHOD_HYBRID, BC_DUCT, 1),
+    ((30, 10, 9), 0.62, METHOD_LEGACY, BC_DUCT, 0),
+]
+
+
+def run_single(steps_list, stats=False, storage=STORE_F32, specs=SPECS):
     out = []
-    for i, spec in enumerate(SPECS):
+    for i, spec in enumerate(specs):
         s = make(spec, i, storage)
         s.enable_stats(stats)
         for n in steps_list:
@@ -87,6 +95,23 @@ def test_narrow_batch_bit_identical_to_single(gpu, storage):
     for i, ((state, sref), s) in enumerate(zip(ref, solvers)):
         np.testing.assert_array_equal(s.state(), state)
         assert st[i, 0] == pytest.approx(sref["mass"], rel=1e-11), i
+    b.close()
+    for s in solvers:
+        s.close()
+
+
+@pytest.mark.parametrize("storage", [STORE_F32, STORE_F16, STORE_BF16])
+def test_any_cell_count_batch_bit_identical_to_single(gpu, storage):
+    """Instances whose cell counts are odd or not multiples of 4: each one's even
+    step takes the vector width its own step takes for that count."""
+    ref = run_single([5, 2], storage=storage, specs=SPECS_ODD)
+    solvers = [make(spec, i, storage) for i, spec in enumerate(SPECS_ODD)]
+    b = Batch(solvers)
+    b.step(5)
+    b.step(2)
+    b.synchronize()
+    for (state, _), s in zip(ref, solvers):
+        np.testing.assert_array_equal(s.state(), state)
     b.close()
     for s in solvers:
         s.close()
@@ -142,12 +167,12 @@ def test_batch_rejects_unsupported_instances(gpu):
     c = Solver(16, 16, 16, 0.6, method=METHOD_LEGACY, storage=STORE_F16)
     d = Solver(16, 16, 16, 0.6, method=METHOD_LEGACY)
     f = Solver(16, 16, 16, 0.6, method=METHOD_LEGACY, storage=STORE_F64)
-    g = Solver(18, 15, 15, 0.6, method=METHOD_LEGACY, storage=STORE_BF16)   # 4050 cells: not a multiple of 4
-    h = Solver(18, 15, 15, 0.6, method=METHOD_LEGACY)                        # even: fine in FP32
-    for bad in ([a], [d, a], [d, c], [f], [g]):
+    g = Solver(18, 15, 15, 0.6, method=METHOD_LEGACY, storage=STORE_BF16)   # 4050 cells: any count is fine
+    h = Solver(17, 15, 15, 0.6, method=METHOD_LEGACY)                        # odd count
+    for bad in ([a], [d, a], [d, c], [f]):
         with pytest.raises(LBMError):
             Batch(bad)
-    for ok in ([c], [h]):
+    for ok in ([c], [g], [h]):
         Batch(ok).close()
     for s in (c, f, g, h):
         s.close()

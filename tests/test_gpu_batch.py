@@ -44,11 +44,12 @@ def make(spec, seed, storage=STORE_F32):
     return s
 
 
-# cell counts that are odd (1575), even but not a multiple of 4 (4050) and a multiple of 4 (2700)
+# cell counts that are odd (1575), even but not a multiple of 4 (4050) and multiples of 4 (2700, 1512)
 SPECS_ODD = [
     ((25, 9, 7), 0.6, METHOD_LEGACY, BC_PERIODIC, 0),
     ((18, 15, 15), 0.57, METHOD_HYBRID, BC_DUCT, 1),
     ((30, 10, 9), 0.62, METHOD_LEGACY, BC_DUCT, 0),
+    ((27, 8, 7), 0.6, METHOD_LEGACY, BC_DUCT, 0),      # odd nx in a duct, 1512 cells
 ]
 
 

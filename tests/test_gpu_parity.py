@@ -200,8 +200,9 @@ def test_home_vs_oracle(gpu, oracle, dims, tau, steps, with_mask, force, bounce)
 
 
 # (30, 10, 9): nx not a multiple of the even step's 4-cell vectors, so vectors
-# run across row ends, where the inlet and outlet cells sit
-@pytest.mark.parametrize("dims", [(40, 18, 14), (136, 10, 8), (30, 10, 9)])
+# run across row ends, where the inlet and outlet cells sit; (31, 10, 9): odd nx
+# (two-cell vectors across row ends; HOME's unpaired last column)
+@pytest.mark.parametrize("dims", [(40, 18, 14), (136, 10, 8), (30, 10, 9), (31, 10, 9)])
 @pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HYBRID, METHOD_HOME])
 def test_duct_vs_oracle(gpu, oracle, method, dims):
     """Velocity inlet / zero-gradient outlet / wall cells / obstacle; drag of the last step."""
@@ -332,8 +333,8 @@ def test_pipelined_host_io_matches_synchronous(gpu, method):
 
 @pytest.mark.parametrize("storage,tol", [(1, 5e-3), (2, 4e-2)])
 @pytest.mark.parametrize("method", [METHOD_LEGACY, METHOD_HYBRID])
-@pytest.mark.parametrize("dims,bc", [((128, 12, 10), BC_DUCT), ((30, 10, 9), BC_DUCT), ((64, 10, 9), BC_PERIODIC),
-                                     ((42, 9, 7), BC_PERIODIC)])
+@pytest.mark.parametrize("dims,bc", [((128, 12, 10), BC_DUCT), ((30, 10, 9), BC_DUCT), ((31, 10, 9), BC_DUCT),
+                                     ((64, 10, 9), BC_PERIODIC), ((42, 9, 7), BC_PERIODIC)])
 def test_narrow_storage_vs_oracle(gpu, oracle, storage, tol, method, dims, bc):
     """F16/BF16 populations (shifted, FP32 arithmetic) against the FP64 oracle:
     duct and periodic grids; cell counts divisible by 4 (four cells per thread

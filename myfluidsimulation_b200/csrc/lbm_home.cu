@@ -224,10 +224,12 @@ __device__ __forceinline__ void static_for(F&& fn) {
 // ---- moment storage: F32 as is; F16/BF16 keep rho - rho0, u and S ---------
 // (F16 scaled by 2^10, exact, as the F16 populations are)
 template <class T> struct MomStore;
+// FP32 moments are read with ld.global.cg (kept in L2, not in L1): each is read
+// once per block, and L1 left free measured 1-3 % faster than the read-only path
 template <> struct MomStore<float> {
     static constexpr float S = 1.0f, invS = 1.0f;
-    __device__ __forceinline__ static float ld(const float* p) { return __ldg(p); }
-    __device__ __forceinline__ static float2 ld2(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+    __device__ __forceinline__ static float ld(const float* p) { return __ldcg(p); }
+    __device__ __forceinline__ static float2 ld2(const float* p) { return __ldcg(reinterpret_cast<const float2*>(p)); }
 };
 template <> struct MomStore<__half> {
     static constexpr float S = kF16Scale, invS = kF16Inv;
